@@ -99,8 +99,15 @@ typedef struct {
   float ms_aggregation;     /* all aggregations */
   float ms_first_optimization;  /* opt0 of the Metrics line */
   float ms_first_aggregation;   /* agg0 of the Metrics line */
-  double bytes_optimization;    /* algorithmic bytes of all optimisation kernels */
-  int64_t reserved[6];
+  double bytes_optimization;    /* algorithmic bytes of the optimisation kernels, summed over
+                                   passes: 12 per active entry + 24 per active vertex */
+  float ms_optimization_kernels;  /* device time of the optimisation kernels only (binning and
+                                     gain evaluation, without apply / modularity) */
+  int32_t reserved1;
+  int64_t kernel_launches;      /* engine kernels launched by the call */
+  int64_t active_entries;       /* sum over passes of the active vertices' entries */
+  int64_t active_vertices;      /* sum over passes of the active vertices */
+  int64_t reserved[3];
 } lv_stats;
 
 typedef struct lv_context lv_context;
@@ -180,6 +187,16 @@ lv_status lv_community_get_best(lv_community* c, int32_t* best);
  * Rows come out sorted by destination, as the reference's sort_by_key leaves them. */
 lv_status lv_community_get_graph(lv_community* c, int64_t* row_ptr, int32_t* col, double* w,
                                  double* k);
+
+/* Per-pass record of a single-graph run: the (I, S, Q) triple compute_modularity prints
+ * after every pass (community.h:102, phaseOptimization.cuh:174-177) plus the move count. */
+typedef struct {
+  int32_t level, iteration, n_moved, reserved;
+  double internal, sum_a2, modularity, delta;
+} lv_trace_record;
+
+/* Copies up to `cap` records (oldest first) and sets *len to the number recorded. */
+lv_status lv_community_get_trace(lv_community* c, lv_trace_record* out, int32_t cap, int32_t* len);
 
 /* ---- serving ---------------------------------------------------------------------------
  * Continuous batching with graph state resident in HBM. No reference counterpart.

@@ -1,0 +1,405 @@
+"""B200 Louvain engine: Python mirror of the reference's host API over the C ABI.
+
+The reference exposes ``ModularityAlgorithms::Louvain(GraphHost&, MODE)`` returning a
+``Community`` (modularityAlgorithms.h:8-10, community.h:15-26). This package keeps those
+names and argument meanings and calls the engine's shared library
+(``liblouvain_b200.so``, C ABI declared in include/louvain_b200.h) through ctypes:
+
+    lv = importlib.import_module("louvain-fast-move-cuda_b200")
+    g = lv.GraphHost("graph.edge", False, 0)          # graphHost.cuh:17
+    C = lv.ModularityAlgorithms.Louvain(g, lv.MODE.SORT)
+    C.best_communities, C.n_of_best_communities, C.modularity
+
+There is no CPU fallback: if the library is missing or no CUDA device is present the calls
+raise ``LouvainError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import graphs as graphs  # noqa: F401
+from .graphs import CSRGraph
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblouvain_b200.so")
+_lib = None
+
+
+class LouvainError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class MODE(enum.IntEnum):
+    """constants.h:13"""
+    HASH = 0
+    SORT = 1
+    ADAPTIVE_SPEED = 2
+    ADAPTIVE_MEMORY = 3
+
+
+MEM_HOST, MEM_DEVICE = 0, 1
+WEIGHTS_AUTO, WEIGHTS_INTEGER, WEIGHTS_FLOAT = 0, 1, 2
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32), ("fast_first", ctypes.c_int32),
+        ("max_iterations", ctypes.c_int32), ("max_levels", ctypes.c_int32),
+        ("threshold", ctypes.c_double), ("chunk_edges", ctypes.c_int64),
+        ("weight_mode", ctypes.c_int32), ("validate", ctypes.c_int32),
+        ("use_graphs", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 7),
+        ("bin_max_degree", ctypes.c_int32 * 8), ("reserved_d", ctypes.c_double * 4),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("modularity", ctypes.c_double), ("n", ctypes.c_int64), ("m", ctypes.c_int64),
+        ("levels", ctypes.c_int32), ("iterations", ctypes.c_int32),
+        ("n_communities", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("ms_total", ctypes.c_float), ("ms_window", ctypes.c_float),
+        ("ms_optimization", ctypes.c_float), ("ms_aggregation", ctypes.c_float),
+        ("ms_first_optimization", ctypes.c_float), ("ms_first_aggregation", ctypes.c_float),
+        ("bytes_optimization", ctypes.c_double), ("ms_optimization_kernels", ctypes.c_float),
+        ("reserved1", ctypes.c_int32), ("kernel_launches", ctypes.c_int64),
+        ("active_entries", ctypes.c_int64), ("active_vertices", ctypes.c_int64),
+        ("reserved", ctypes.c_int64 * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+class CommunityInfo(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int64), ("E", ctypes.c_int64), ("n0", ctypes.c_int64),
+        ("level", ctypes.c_int32), ("iteration", ctypes.c_int32),
+        ("modularity", ctypes.c_double), ("internal", ctypes.c_double),
+        ("sum_a2", ctypes.c_double), ("total_weight", ctypes.c_double),
+        ("n_best", ctypes.c_int64), ("weights_integer", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+TRACE_DTYPE = np.dtype([
+    ("level", np.int32), ("iteration", np.int32), ("n_moved", np.int32), ("reserved", np.int32),
+    ("internal", np.float64), ("sum_a2", np.float64), ("modularity", np.float64),
+    ("delta", np.float64),
+])
+
+# Every entry point the header declares; tests check that the library exports all of them.
+EXPORTS = (
+    "lv_config_default", "lv_create", "lv_destroy", "lv_last_error", "lv_status_string",
+    "lv_abi_version", "lv_run_csr", "lv_run_batch", "lv_community_create",
+    "lv_community_destroy", "lv_optimization_step", "lv_optimization_run",
+    "lv_aggregation_run", "lv_louvain", "lv_community_info_get", "lv_community_get_partition",
+    "lv_community_get_best", "lv_community_get_graph", "lv_community_get_trace",
+    "lv_server_create", "lv_server_destroy", "lv_server_submit", "lv_server_progress",
+    "lv_server_poll", "lv_server_drain",
+)
+
+
+def load_library(path: Optional[str] = None):
+    """Load liblouvain_b200.so (built by ``make -C louvain-fast-move-cuda_b200/csrc``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise LouvainError(-1, f"engine library not built: {p} is missing "
+                               "(run `make -C louvain-fast-move-cuda_b200/csrc` or __graft_entry__.build())")
+    L = ctypes.CDLL(p)
+    vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P = ctypes.POINTER
+    sig = {
+        "lv_config_default": (None, [P(Config)]),
+        "lv_create": (i32, [i32, P(Config), P(vp)]),
+        "lv_destroy": (i32, [vp]),
+        "lv_last_error": (ctypes.c_char_p, [vp]),
+        "lv_status_string": (ctypes.c_char_p, [i32]),
+        "lv_abi_version": (i32, []),
+        "lv_run_csr": (i32, [vp, i64, vp, vp, vp, i32, vp, i32, P(dbl), P(Stats)]),
+        "lv_run_batch": (i32, [vp, i32, vp, vp, vp, vp, i32, vp, i32, vp, vp, P(Stats)]),
+        "lv_community_create": (i32, [vp, i64, vp, vp, vp, i32, P(vp)]),
+        "lv_community_destroy": (i32, [vp]),
+        "lv_optimization_step": (i32, [vp, P(dbl), P(i64)]),
+        "lv_optimization_run": (i32, [vp, P(i32)]),
+        "lv_aggregation_run": (i32, [vp, i32]),
+        "lv_louvain": (i32, [vp, P(Stats)]),
+        "lv_community_info_get": (i32, [vp, P(CommunityInfo)]),
+        "lv_community_get_partition": (i32, [vp, vp, vp]),
+        "lv_community_get_best": (i32, [vp, vp]),
+        "lv_community_get_graph": (i32, [vp, vp, vp, vp, vp]),
+        "lv_community_get_trace": (i32, [vp, vp, i32, P(i32)]),
+        "lv_server_create": (i32, [vp, i64, i32, P(vp)]),
+        "lv_server_destroy": (i32, [vp]),
+        "lv_server_submit": (i32, [vp, i64, vp, vp, vp, P(i64)]),
+        "lv_server_progress": (i32, [vp, P(i64), P(i64), P(i64)]),
+        "lv_server_poll": (i32, [vp, i64, vp, P(dbl), P(dbl), P(i32)]),
+        "lv_server_drain": (i32, [vp]),
+    }
+    missing = []
+    for name, (res, args) in sig.items():
+        try:
+            fn = getattr(L, name)
+        except AttributeError:
+            missing.append(name)
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    L.missing_exports = tuple(missing)
+    if path is None:
+        _lib = L
+    return L
+
+
+def _ptr(a) -> Optional[int]:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor
+
+
+def _is_device(a) -> bool:
+    return a is not None and not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+def config(mode: int = MODE.SORT, threshold: float = 1e-3, fast_first: bool = True,
+           chunk_edges: int = 50_000_000, max_iterations: int = 1_000_000_000,
+           max_levels: int = 0, weight_mode: int = WEIGHTS_AUTO,
+           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = True) -> Config:
+    c = Config()
+    load_library().lv_config_default(ctypes.byref(c))
+    c.mode = int(mode)
+    c.threshold = float(threshold)
+    c.fast_first = int(bool(fast_first))
+    c.chunk_edges = int(chunk_edges)
+    c.max_iterations = int(max_iterations)
+    c.max_levels = int(max_levels)
+    c.weight_mode = int(weight_mode)
+    c.use_graphs = int(bool(use_graphs))
+    if bin_max_degree is not None:
+        for i, d in enumerate(bin_max_degree[:8]):
+            c.bin_max_degree[i] = int(d)
+    return c
+
+
+class Engine:
+    """An lv_context: one device, its stream and reusable state."""
+
+    def __init__(self, device: int = 0, cfg: Optional[Config] = None, **kw):
+        self._L = load_library()
+        self.cfg = cfg if cfg is not None else config(**kw)
+        h = ctypes.c_void_p()
+        st = self._L.lv_create(int(device), ctypes.byref(self.cfg), ctypes.byref(h))
+        if st != 0:
+            raise LouvainError(st, "lv_create failed: " + self._L.lv_status_string(st).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def check(self, st: int, what: str):
+        if st != 0:
+            msg = self._L.lv_last_error(self._h).decode() or self._L.lv_status_string(st).decode()
+            raise LouvainError(st, f"{what}: {msg}")
+
+    # -- one-shot --------------------------------------------------------------------------
+    def run_csr(self, n: int, row_ptr, col, w=None, out=None, stats: bool = True):
+        """lv_run_csr on numpy (host) or torch CUDA (device) arrays. Returns
+        (communities, modularity, Stats)."""
+        dev = _is_device(row_ptr)
+        if not dev:
+            row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+        if out is None:
+            out = np.empty(n, dtype=np.int32)
+        q = ctypes.c_double(0)
+        s = Stats()
+        st = self._L.lv_run_csr(self._h, int(n), _ptr(row_ptr), _ptr(col), _ptr(w),
+                                MEM_DEVICE if dev else MEM_HOST, _ptr(out),
+                                MEM_DEVICE if _is_device(out) else MEM_HOST,
+                                ctypes.byref(q), ctypes.byref(s) if stats else None)
+        self.check(st, "lv_run_csr")
+        return out, q.value, s
+
+    def run_graph(self, g: CSRGraph):
+        return self.run_csr(g.n, g.row_ptr, g.col, g.w)
+
+    def run_batch(self, vtx_offsets, row_ptr, col, w=None, out=None):
+        """lv_run_batch: returns (communities, modularity[G], n_communities[G], Stats)."""
+        dev = _is_device(row_ptr)
+        if not dev:
+            vtx_offsets = np.ascontiguousarray(vtx_offsets, dtype=np.int64)
+            row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+            G = vtx_offsets.size - 1
+            n = int(vtx_offsets[-1])
+        else:
+            G = int(vtx_offsets.numel()) - 1
+            n = int(vtx_offsets[-1].item())
+        if out is None:
+            out = np.empty(n, dtype=np.int32)
+        qs = np.empty(G, dtype=np.float64)
+        ks = np.empty(G, dtype=np.int32)
+        s = Stats()
+        st = self._L.lv_run_batch(self._h, G, _ptr(vtx_offsets), _ptr(row_ptr), _ptr(col), _ptr(w),
+                                  MEM_DEVICE if dev else MEM_HOST, _ptr(out),
+                                  MEM_DEVICE if _is_device(out) else MEM_HOST,
+                                  qs.ctypes.data, ks.ctypes.data, ctypes.byref(s))
+        self.check(st, "lv_run_batch")
+        return out, qs, ks, s
+
+    def community(self, g: CSRGraph) -> "CommunityState":
+        return CommunityState(self, g)
+
+
+class CommunityState:
+    """Phase-level handle (lv_community): the reference's Community plus the phase calls
+    OptimizationPhase::run / AggregationPhase::run that modularity_routine makes."""
+
+    def __init__(self, engine: Engine, g: CSRGraph):
+        self.e = engine
+        self._row = np.ascontiguousarray(g.row_ptr, dtype=np.int64)
+        self._col = np.ascontiguousarray(g.col, dtype=np.int32)
+        self._w = None if g.w is None else np.ascontiguousarray(g.w, dtype=np.float32)
+        h = ctypes.c_void_p()
+        st = engine._L.lv_community_create(engine._h, g.n, _ptr(self._row), _ptr(self._col),
+                                           _ptr(self._w), MEM_HOST, ctypes.byref(h))
+        engine.check(st, "lv_community_create")
+        self._h = h
+        self.n0 = g.n
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.e._L.lv_community_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def optimization_step(self):
+        d = ctypes.c_double(0)
+        mv = ctypes.c_int64(0)
+        self.e.check(self.e._L.lv_optimization_step(self._h, ctypes.byref(d), ctypes.byref(mv)),
+                     "lv_optimization_step")
+        return int(mv.value), d.value
+
+    def optimization_run(self) -> int:
+        it = ctypes.c_int32(0)
+        self.e.check(self.e._L.lv_optimization_run(self._h, ctypes.byref(it)), "lv_optimization_run")
+        return it.value
+
+    def aggregation_run(self, aggregate: bool) -> None:
+        self.e.check(self.e._L.lv_aggregation_run(self._h, int(bool(aggregate))), "lv_aggregation_run")
+
+    def louvain(self) -> Stats:
+        s = Stats()
+        self.e.check(self.e._L.lv_louvain(self._h, ctypes.byref(s)), "lv_louvain")
+        return s
+
+    def info(self) -> CommunityInfo:
+        i = CommunityInfo()
+        self.e.check(self.e._L.lv_community_info_get(self._h, ctypes.byref(i)), "lv_community_info_get")
+        return i
+
+    def partition(self):
+        n = self.info().n
+        comm = np.empty(n, dtype=np.int32)
+        tot = np.empty(n, dtype=np.float64)
+        self.e.check(self.e._L.lv_community_get_partition(self._h, comm.ctypes.data, tot.ctypes.data),
+                     "lv_community_get_partition")
+        return comm, tot
+
+    def best(self) -> np.ndarray:
+        out = np.empty(self.n0, dtype=np.int32)
+        self.e.check(self.e._L.lv_community_get_best(self._h, out.ctypes.data), "lv_community_get_best")
+        return out
+
+    def graph(self):
+        i = self.info()
+        row = np.empty(i.n + 1, dtype=np.int64)
+        col = np.empty(max(i.E, 1), dtype=np.int32)
+        w = np.empty(max(i.E, 1), dtype=np.float64)
+        k = np.empty(max(i.n, 1), dtype=np.float64)
+        self.e.check(self.e._L.lv_community_get_graph(self._h, row.ctypes.data, col.ctypes.data,
+                                                      w.ctypes.data, k.ctypes.data),
+                     "lv_community_get_graph")
+        return row, col[: i.E], w[: i.E], k[: i.n]
+
+    def trace(self) -> np.ndarray:
+        cap = 4096
+        out = np.empty(cap, dtype=TRACE_DTYPE)
+        ln = ctypes.c_int32(0)
+        self.e.check(self.e._L.lv_community_get_trace(self._h, out.ctypes.data, cap, ctypes.byref(ln)),
+                     "lv_community_get_trace")
+        return out[: min(ln.value, cap)]
+
+
+# ---- the reference's own names -------------------------------------------------------------------
+class GraphHost:
+    """graphHost.cuh:7-18. ``GraphHost(name, weighted, skip_line)`` parses an ``a b`` edge list
+    like graph.cu:17-87; ``GraphHost.from_csr(g)`` wraps an in-memory CSRGraph."""
+
+    def __init__(self, name: Optional[str] = None, weighted: bool = False, skip_line: int = 0,
+                 csr: Optional[CSRGraph] = None):
+        if csr is None:
+            if weighted:
+                raise LouvainError(2, "weighted edge lists are not parsed (the reference's "
+                                      "weighted branch is a TODO, graph.cu:32-34); pass a CSRGraph")
+            csr = graphs.read_edge_list(name, skip_line)
+        self.csr = csr
+        self.n_nodes = csr.n
+        self.n_links = csr.m
+        self.total_weight = float(csr.weights_or_ones.sum()) / 2.0
+        self.min_id = 0
+
+    @classmethod
+    def from_csr(cls, g: CSRGraph) -> "GraphHost":
+        return cls(csr=g)
+
+
+class Community:
+    """community.h:15-26: the result of a Louvain run."""
+
+    def __init__(self, best, n_best: int, modularity: float, stats: Optional[Stats] = None):
+        self.best_communities = best
+        self.n_of_best_communities = int(n_best)
+        self.modularity = float(modularity)
+        self.stats = stats
+
+
+_engines = {}
+
+
+def _engine_for(mode: int, **kw) -> Engine:
+    key = (int(mode), tuple(sorted(kw.items())))
+    if key not in _engines:
+        _engines[key] = Engine(0, mode=mode, **kw)
+    return _engines[key]
+
+
+class ModularityAlgorithms:
+    """modularityAlgorithms.h:7-82."""
+
+    @staticmethod
+    def Louvain(graph: GraphHost, fastLocalMoveEnable: int = MODE.SORT, **kw) -> Community:
+        g = graph.csr if isinstance(graph, GraphHost) else graph
+        e = _engine_for(int(fastLocalMoveEnable), **kw)
+        best, q, s = e.run_graph(g)
+        return Community(best, s.n_communities, q, s)

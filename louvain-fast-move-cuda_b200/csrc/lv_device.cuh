@@ -1,0 +1,235 @@
+// lv_device.cuh -- device-side building blocks of the B200 Louvain engine: state layout,
+// the reference's gain arithmetic, shared-memory hash tables, argmax keys, warp/block
+// reductions and scans.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lv {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;  // empty hash slot / no community
+constexpr uint32_t kNever = 0xFFFFFFFFu;  // iteration stamp that never matches
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Per-graph phase inside a batch.
+enum : uint32_t { kIterating = 0, kLevelDone = 1, kFinished = 2 };
+
+// Device error bits (lv_status LV_ERR_DEVICE_CHECK carries them).
+enum : uint32_t {
+  kErrTableFull = 1u << 0,    // a hash insert ran out of probes
+  kErrArena = 1u << 1,        // a global table slice beyond the arena
+  kErrIndex = 1u << 2,        // checked build: an index out of range
+  kErrInput = 1u << 3,        // input validation: col out of range / empty row / bad weight
+  kErrChunks = 1u << 4,       // more edge chunks than the emulation supports
+  kErrRange = 1u << 5,        // integer mode: total weight >= 2^32
+};
+
+constexpr int kMaxChunks = 1024;
+constexpr int kNumBins = 8;
+constexpr int kTraceCap = 4096;
+
+// Per-graph state (one entry per graph of a batch; a single run has one).
+struct GraphState {
+  double m;           // total_weight, fixed at level 0 (graph.cu:81)
+  double two_m2;      // (2*m)*m, the denominator as operatorsDelta.h:40 evaluates it
+  double Q;           // Community::modularity
+  double Q_level;     // modularity at the start of the current level
+  unsigned long long I;  // internal weight: u64 (integer mode) or double bits (float mode)
+  unsigned long long S;  // sum of squared totals: u64 or double bits
+  uint32_t phase;
+  uint32_t iters;     // passes in the current level
+  uint32_t level;
+  uint32_t n_best;    // n_of_best_communities
+  uint32_t vb, ve;    // vertex range in the current level
+  uint32_t cont;      // aggregation: contract (1) or finish (0)
+  uint32_t agg;       // taking part in the running aggregation
+  uint32_t map_base;  // aggregation: nonempty communities before this graph
+  uint32_t total_iters;
+  uint32_t moved;     // moves of the last pass
+  uint32_t pad;
+};
+
+struct TraceRec {
+  uint32_t level, iteration, n_moved, pad;
+  double internal, sum_a2, modularity, delta;
+};
+
+// Device control block: counters, loop state and the active-pass description. Kernels read
+// sizes and the iteration stamp from here so that a captured graph can be replayed.
+struct Ctrl {
+  uint32_t it;                 // global pass stamp
+  uint32_t n, E;               // current level sizes
+  uint32_t n0;                 // original vertices
+  uint32_t G;                  // graphs
+  uint32_t n_iterating;        // graphs still in kIterating after the last pass
+  uint32_t err;
+  uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
+  uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
+  uint32_t bin_count[kNumBins];
+  uint32_t mover_count;
+  uint32_t hub_cursor;         // global hash-table arena cursor (slots)
+  uint32_t arena_slots;        // arena capacity (slots)
+  uint32_t n_next, E_next;     // aggregation outputs
+  uint32_t n_chunks;           // chunk early-return emulation (single graph)
+  uint32_t chunk_lo[kMaxChunks + 1];
+  uint32_t chunk_any[kMaxChunks];
+  uint32_t chunk_on;           // emulation active for this level
+  uint32_t loop_continue;      // device-side loop control for captured graphs
+  uint32_t trace_len;
+  uint32_t pass;               // pass index inside the current level
+  uint32_t max_iterations;
+  uint32_t act_vertices;       // this pass: vertices binned (active and considered)
+  unsigned long long act_entries;         // this pass: their entries
+  unsigned long long act_vertices_total;  // summed over the run's passes
+  unsigned long long act_entries_total;
+  double threshold;
+  TraceRec trace[kTraceCap];
+};
+
+// ---- reference arithmetic -----------------------------------------------------------------
+// operatorsDelta.h:29-45 (DeltaModularitySort / DeltaModularityHash): the float difference
+// w_vc - self_v, then double: diff/m + k*(a_own - k - a_c)/((2m)m), rounded to float. The
+// explicit _rn intrinsics keep every step a single IEEE rounding (no FMA contraction), so the
+// result is bit-identical to the reference and to the oracle.
+__device__ __forceinline__ float gain_ref(float w_vc, float self_v, double k, double a_own,
+                                          double a_c, double m, double two_m2) {
+  const float diff = __fsub_rn(w_vc, self_v);
+  const double t1 = __ddiv_rn((double)diff, m);
+  const double t2 = __ddiv_rn(__dmul_rn(k, __dsub_rn(__dsub_rn(a_own, k), a_c)), two_m2);
+  return __double2float_rn(__dadd_rn(t1, t2));
+}
+
+// Argmax key for a positive gain: the float bits order positive floats, the low word breaks
+// ties -- ~c makes the lowest community win (SORT: GetMaxValue keeps the first of equal
+// values in ascending community order, operators.h:30-40), c makes the highest win (HASH:
+// atomicMax of (gain bits << 32 | c), phaseOptimizationHash.cu:23-35). 0 = no candidate.
+__device__ __forceinline__ unsigned long long argmax_key(float g, uint32_t c, bool lowest) {
+  return ((unsigned long long)__float_as_uint(g) << 32) | (lowest ? (uint32_t)~c : c);
+}
+__device__ __forceinline__ uint32_t key_comm(unsigned long long key, bool lowest) {
+  const uint32_t lo = (uint32_t)key;
+  return lowest ? ~lo : lo;
+}
+__device__ __forceinline__ float key_gain(unsigned long long key) {
+  return __uint_as_float((uint32_t)(key >> 32));
+}
+
+// ---- weight types ----------------------------------------------------------------------------
+// Integer mode keeps u32 weights and exact u32/u64 sums (the reference's `unsigned` weights);
+// float mode keeps fp32 weights and double sums.
+template <bool WINT> struct WTraits;
+template <> struct WTraits<true> {
+  using W = uint32_t;
+  using Acc = uint32_t;  // a row's weight sum is at most k_v <= 2m < 2^32
+  __device__ static __forceinline__ float to_float(Acc x) { return __uint2float_rn(x); }
+  __device__ static __forceinline__ float w_float(W x) { return __uint2float_rn(x); }
+  __device__ static __forceinline__ double w_double(W x) { return (double)x; }
+};
+template <> struct WTraits<false> {
+  using W = float;
+  using Acc = double;
+  __device__ static __forceinline__ float to_float(Acc x) { return __double2float_rn(x); }
+  __device__ static __forceinline__ float w_float(W x) { return x; }
+  __device__ static __forceinline__ double w_double(W x) { return (double)x; }
+};
+
+// ---- hashing -------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t hash_slot(uint32_t c, uint32_t shift) {
+  return (c * 2654435761u) >> shift;
+}
+__device__ __forceinline__ uint32_t log2_pow2(uint32_t x) { return 31u - __clz(x); }
+__host__ __device__ __forceinline__ uint32_t next_pow2(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+__device__ __forceinline__ void acc_add(uint32_t* p, uint32_t v) { atomicAdd(p, v); }
+__device__ __forceinline__ void acc_add(double* p, double v) { atomicAdd(p, v); }
+
+// Open addressing with linear probing; keys go EMPTY -> c once and never change again, so a
+// non-empty slot read is final. Capacity >= 2 x inserts, so the probe bound is never reached
+// in a correctly sized table; reaching it reports kErrTableFull instead of looping.
+template <class Acc>
+__device__ __forceinline__ bool table_add(uint32_t* keys, Acc* vals, uint32_t mask,
+                                          uint32_t shift, uint32_t c, Acc w) {
+  uint32_t h = hash_slot(c, shift);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    uint32_t cur = ((volatile uint32_t*)keys)[h];
+    if (cur == kEmpty) {
+      cur = atomicCAS(&keys[h], kEmpty, c);
+      if (cur == kEmpty) cur = c;
+    }
+    if (cur == c) {
+      acc_add(&vals[h], w);
+      return true;
+    }
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+template <class Acc>
+__device__ __forceinline__ Acc table_get(const uint32_t* keys, const Acc* vals, uint32_t mask,
+                                         uint32_t shift, uint32_t c) {
+  uint32_t h = hash_slot(c, shift);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t cur = keys[h];
+    if (cur == c) return vals[h];
+    if (cur == kEmpty) return Acc(0);
+    h = (h + 1) & mask;
+  }
+  return Acc(0);
+}
+
+// ---- warp / block reductions -------------------------------------------------------------------
+template <int T>
+__device__ __forceinline__ unsigned long long team_max(unsigned long long x, unsigned mask) {
+#pragma unroll
+  for (int o = T / 2; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(mask, x, o);
+    x = y > x ? y : x;
+  }
+  return x;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_incl_scan(T x, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// Exclusive block scan; every thread of the block must call it. `sh` holds >= 33 T.
+template <class T, int NT>
+__device__ __forceinline__ T block_excl_scan(T x, T* sh, T* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const T inc = warp_incl_scan(x, lane);
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    T s = lane < NT / 32 ? sh[lane] : T(0);
+    s = warp_incl_scan(s, lane);
+    if (lane < NT / 32) sh[lane] = s;
+    if (lane == NT / 32 - 1) sh[32] = s;
+  }
+  __syncthreads();
+  const T base = wid > 0 ? sh[wid - 1] : T(0);
+  if (total) *total = sh[32];
+  const T out = base + inc - x;
+  __syncthreads();
+  return out;
+}
+
+}  // namespace lv

@@ -1,0 +1,924 @@
+// lv_engine.cu -- host side of the B200 Louvain engine and its C ABI (include/louvain_b200.h).
+//
+// A Run holds one batch of graphs (a single-graph call is a batch of one) resident in HBM:
+// the current level's CSR, the partition state and all scratch, allocated once at level-0
+// size and reused by every level (the reference allocates 6 x STEP_ROUND vectors per level,
+// phaseOptimization.cuh:50-68, and 2E entries per modularity evaluation, community.h:69,85).
+// The level loop mirrors ModularityAlgorithms::modularity_routine (modularityAlgorithms.h:
+// 14-81); each pass is a fixed kernel sequence whose sizes live on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/louvain_b200.h"
+#include "lv_kernels.cuh"
+
+// A context keeps the device memory of finished runs in a pool and hands it to the next run,
+// so repeated calls allocate nothing (cudaMalloc / cudaFree synchronise the whole device).
+struct lv_context {
+  int device = 0;
+  lv_config cfg{};
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::mutex mu;
+  std::multimap<size_t, void*> pool;  // free device blocks by size
+  size_t pool_bytes = 0;
+  std::mutex pool_mu;                 // runs of the serving loop allocate concurrently
+  uint32_t* pinned = nullptr;         // small host readbacks
+  cudaEvent_t ev[8] = {};
+
+  // A pooled block of at least `bytes` (and not wastefully larger), or nullptr; *got = its size.
+  void* take(size_t bytes, size_t* got) {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    auto it = pool.lower_bound(bytes);
+    if (it != pool.end() && it->first <= bytes * 2 + (1u << 20)) {
+      void* p = it->second;
+      *got = it->first;
+      pool_bytes -= it->first;
+      pool.erase(it);
+      return p;
+    }
+    return nullptr;
+  }
+  void give(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    pool.emplace(bytes, p);
+    pool_bytes += bytes;
+  }
+  void drain_pool() {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    for (auto& kv : pool) cudaFree(kv.second);
+    pool.clear();
+    pool_bytes = 0;
+  }
+  bool pool_empty() {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    return pool.empty();
+  }
+};
+
+namespace lv {
+
+static const char* kStatusText[] = {
+    "ok", "invalid argument", "invalid input graph", "size or weight beyond the supported range",
+    "CUDA error", "out of memory", "device-side check failed", "request exceeds the memory budget",
+    "invalid state"};
+
+struct Fail {
+  lv_status st;
+  std::string msg;
+};
+
+#define LV_CUDA(call)                                                                 \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      throw Fail{e_ == cudaErrorMemoryAllocation ? LV_ERR_NOMEM : LV_ERR_CUDA,        \
+                 std::string(#call) + ": " + cudaGetErrorString(e_)};                 \
+  } while (0)
+
+// Default degree bins: team sizes 4/8/16/32 lanes with tables of 2x the bin's maximum
+// degree, a block per vertex up to 8192 entries (16K-slot shared table), global tables above.
+static const uint32_t kDefaultMaxDeg[kNumBins] = {4, 8, 16, 32, 128, 512, 8192, 0xFFFFFFFFu};
+static const int kTeamT[6] = {4, 8, 16, 32, 32, 32};
+
+struct Block {
+  void* p;
+  size_t bytes;
+};
+
+// Device allocation through the context's pool; blocks go back to the pool when the run ends.
+template <class T>
+static T* dalloc(lv_context* ctx, std::vector<Block>& owned, size_t count) {
+  if (count == 0) count = 1;
+  const size_t bytes = ((count * sizeof(T) + 255) / 256) * 256;
+  size_t got = bytes;
+  void* p = ctx->take(bytes, &got);
+  if (!p) {
+    got = bytes;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation && !ctx->pool_empty()) {
+      cudaGetLastError();
+      ctx->drain_pool();
+      e = cudaMalloc(&p, bytes);
+    }
+    LV_CUDA(e);
+  }
+  owned.push_back({p, got});
+  return reinterpret_cast<T*>(p);
+}
+
+struct HostCtrlSnap {
+  uint32_t it, n, E, n0, G, n_iterating, err, fast, rule_sort;
+};
+
+class Run {
+ public:
+  lv_context* ctx;
+  lv_config cfg;
+  bool wint = true;
+  uint32_t G = 1;
+  uint32_t n0 = 0, n = 0, E = 0;
+  int64_t m_edges = 0;
+  Dev D{};
+  BinCfg bins{};
+  std::vector<Block> owned;
+  uint64_t arena_slots = 0;
+  int grid_n = 0;           // blocks for vertex-parallel kernels
+  int grid_sq = 0;          // blocks of k_commit_sq (partials)
+  int grid_team[6] = {0};
+  int grid_block[2] = {0};
+  uint32_t team_cap[6] = {0};
+  uint32_t block_cap = 0;
+  cudaStream_t st;
+  uint32_t* pinned = nullptr;  // small readbacks (64 bytes of pinned host memory)
+  bool own_pinned = false;
+  bool finished = false;
+  int32_t levels_run = 0;
+  double t_opt_ms = 0, t_agg_ms = 0, t_opt0 = -1, t_agg0 = -1, t_optk_ms = 0;
+  int64_t launches = 0;
+  cudaEvent_t ev[6];
+  std::vector<Block> arena_blocks;
+
+  // stream == nullptr: the context's stream and readback buffer (calls serialised by the
+  // context lock); otherwise a private stream, as the serving loop runs several at once.
+  explicit Run(lv_context* c, cudaStream_t stream = nullptr) : ctx(c), cfg(c->cfg) {
+    for (auto& e : ev) e = nullptr;
+    st = stream ? stream : c->stream;
+    if (stream) {
+      own_pinned = true;
+    } else {
+      pinned = c->pinned;
+    }
+  }
+  ~Run() {
+    cudaStreamSynchronize(st);
+    for (const Block& b : owned) ctx->give(b.p, b.bytes);
+    for (const Block& b : arena_blocks) ctx->give(b.p, b.bytes);
+    if (own_pinned && pinned) cudaFreeHost(pinned);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+
+  bool single() const { return G == 1; }
+  size_t acc_size() const { return wint ? 4 : 8; }
+
+  void sync() { LV_CUDA(cudaStreamSynchronize(st)); }
+
+  template <class T>
+  T read_ctrl(size_t offset) {
+    LV_CUDA(cudaMemcpyAsync(pinned, reinterpret_cast<char*>(D.ctrl) + offset, sizeof(T),
+                            cudaMemcpyDeviceToHost, st));
+    sync();
+    T v;
+    std::memcpy(&v, pinned, sizeof(T));
+    return v;
+  }
+  uint32_t ctrl_u32(size_t offset) { return read_ctrl<uint32_t>(offset); }
+  void write_ctrl_u32(size_t offset, uint32_t v) {
+    LV_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(D.ctrl) + offset, &v, 4, cudaMemcpyHostToDevice, st));
+    sync();
+  }
+
+  void check_device_errors() {
+    const uint32_t e = ctrl_u32(offsetof(Ctrl, err));
+    LV_CUDA(cudaGetLastError());
+    if (e & kErrInput) throw Fail{LV_ERR_INPUT, "input graph: a row is empty, a column index is outside its graph, or a weight is invalid for the weight mode"};
+    if (e & kErrRange) throw Fail{LV_ERR_RANGE, "integer weights: total weight 2m must be below 2^32 (the reference sums in u32)"};
+    if (e) throw Fail{LV_ERR_DEVICE_CHECK, "device check failed (flags " + std::to_string(e) + ")"};
+  }
+
+  // ---- setup ------------------------------------------------------------------------------------
+  void setup_bins() {
+    for (int b = 0; b < kNumBins; ++b)
+      bins.maxdeg[b] = cfg.bin_max_degree[b] > 0 ? (uint32_t)cfg.bin_max_degree[b] : kDefaultMaxDeg[b];
+    bins.maxdeg[kNumBins - 1] = 0xFFFFFFFFu;
+    for (int b = 0; b + 1 < kNumBins; ++b)
+      if (bins.maxdeg[b + 1] < bins.maxdeg[b]) throw Fail{LV_ERR_ARGUMENT, "bin_max_degree must be non-decreasing"};
+    for (int b = 0; b < 6; ++b) team_cap[b] = next_pow2(2u * std::max(1u, bins.maxdeg[b]));
+    block_cap = next_pow2(2u * std::max(1u, bins.maxdeg[6]));
+    const size_t slot = 4 + acc_size();
+    int max_smem = 0;
+    LV_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    if ((size_t)block_cap * slot > (size_t)max_smem - 1024)
+      throw Fail{LV_ERR_ARGUMENT, "bin 6 table does not fit shared memory"};
+    for (int b = 0; b < 6; ++b)
+      if ((size_t)(256 / kTeamT[b]) * team_cap[b] * slot > (size_t)max_smem - 1024)
+        throw Fail{LV_ERR_ARGUMENT, "team bin table does not fit shared memory"};
+  }
+
+  template <int T>
+  void team_grid(int b, const void* opt_fn, const void* con_fn) {
+    const size_t smem = (size_t)(256 / T) * team_cap[b] * (4 + acc_size());
+    LV_CUDA(cudaFuncSetAttribute(opt_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LV_CUDA(cudaFuncSetAttribute(con_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, opt_fn, 256, smem));
+    grid_team[b] = ctx->sms * std::max(1, occ);
+  }
+
+  template <bool WI>
+  void configure_kernels() {
+    team_grid<4>(0, (const void*)k_opt_team<4, WI>, (const void*)k_contract_team<4, WI>);
+    team_grid<8>(1, (const void*)k_opt_team<8, WI>, (const void*)k_contract_team<8, WI>);
+    team_grid<16>(2, (const void*)k_opt_team<16, WI>, (const void*)k_contract_team<16, WI>);
+    team_grid<32>(3, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    const size_t bsmem = (size_t)block_cap * (4 + acc_size());
+    LV_CUDA(cudaFuncSetAttribute((const void*)k_opt_block<WI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    LV_CUDA(cudaFuncSetAttribute((const void*)k_contract_block<WI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    int occ = 0;
+    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, false>, 512, bsmem));
+    grid_block[0] = ctx->sms * std::max(1, occ);
+    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, true>, 512, 0));
+    grid_block[1] = ctx->sms * std::max(1, occ);
+  }
+
+  // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
+  void init(uint32_t G_, const int64_t* offs, int64_t n_, const int64_t* row_ptr, const int32_t* col,
+            const float* w, int in_mem) {
+    if (n_ <= 0 || !row_ptr || !col) throw Fail{LV_ERR_ARGUMENT, "n must be positive; row_ptr and col are required"};
+    if (n_ >= 0xFFFFFFFFll) throw Fail{LV_ERR_RANGE, "more than 2^32-2 vertices"};
+    G = G_;
+    n0 = n = (uint32_t)n_;
+    const cudaMemcpyKind kin = in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    int64_t E64 = 0;
+    LV_CUDA(cudaMemcpyAsync(&E64, row_ptr + n_, sizeof(int64_t),
+                            in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, st));
+    sync();
+    if (E64 <= 0) throw Fail{LV_ERR_INPUT, "graph has no edges"};
+    // hash tables are sized next_pow2(2 x row length) in u32 arithmetic
+    if (E64 > (1ll << 30)) throw Fail{LV_ERR_RANGE, "more than 2^30 edge entries"};
+    E = (uint32_t)E64;
+    m_edges = E64 / 2;
+    if (own_pinned) LV_CUDA(cudaMallocHost(&pinned, 64));
+    for (auto& e : ev) LV_CUDA(cudaEventCreate(&e));
+
+    // device arrays (level-0 sizes, reused by every level)
+    D.row = dalloc<uint32_t>(ctx, owned,n + 1);
+    D.rowB = dalloc<uint32_t>(ctx, owned,n + 1);
+    D.col = dalloc<uint32_t>(ctx, owned,E);
+    D.colB = dalloc<uint32_t>(ctx, owned,E);
+    D.w = dalloc<uint32_t>(ctx, owned,E);
+    D.wB = dalloc<uint32_t>(ctx, owned,E);
+    D.k = dalloc<double>(ctx, owned,n);
+    D.kB = dalloc<double>(ctx, owned,n);
+    D.comm = dalloc<uint32_t>(ctx, owned,n);
+    D.a = dalloc<double>(ctx, owned,n);
+    D.new_comm = dalloc<uint32_t>(ctx, owned,n);
+    D.moved_it = dalloc<uint32_t>(ctx, owned,n);
+    D.active_it = dalloc<uint32_t>(ctx, owned,n);
+    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned,n);
+    D.hub_off = dalloc<uint32_t>(ctx, owned,n);
+    D.movers = dalloc<uint32_t>(ctx, owned,n);
+    D.gs = dalloc<GraphState>(ctx, owned,G);
+    D.ctrl = dalloc<Ctrl>(ctx, owned,1);
+    D.partials = dalloc<double>(ctx, owned,kMaxPartials);
+    D.map = dalloc<unsigned long long>(ctx, owned,n);
+    D.cd = dalloc<unsigned long long>(ctx, owned,(size_t)n + 1);
+    D.rank = dalloc<uint32_t>(ctx, owned,n);
+    D.members = dalloc<uint32_t>(ctx, owned,n);
+    D.newdeg = dalloc<uint32_t>(ctx, owned,(size_t)n + 1);
+    D.best = dalloc<uint32_t>(ctx, owned,n0);
+    D.out = dalloc<int32_t>(ctx, owned,n0);
+    if (G > 1) {
+      D.gid = dalloc<uint32_t>(ctx, owned,n);
+      D.gidB = dalloc<uint32_t>(ctx, owned,n);
+      D.gid0 = dalloc<uint32_t>(ctx, owned,n0);
+    }
+    scan_tmp = dalloc<unsigned long long>(ctx, owned,(size_t)(n + 1) / kScanTile + 2);
+    scan_tot = dalloc<unsigned long long>(ctx, owned,1);
+
+    // weight mode
+    float* w_dev_tmp = nullptr;
+    if (w) {
+      LV_CUDA(cudaMemcpyAsync(D.w, w, (size_t)E * 4, kin, st));
+      w_dev_tmp = reinterpret_cast<float*>(D.w);
+    }
+    int wm = cfg.weight_mode;
+    if (!w) wm = LV_WEIGHTS_INTEGER;
+    if (wm == LV_WEIGHTS_AUTO) {
+      uint32_t* flag = reinterpret_cast<uint32_t*>(D.partials);
+      LV_CUDA(cudaMemsetAsync(flag, 0, 4, st));
+      k_weights_integral<<<ctx->sms * 4, 256, 0, st>>>(w_dev_tmp, E, flag);
+      LV_CUDA(cudaMemcpyAsync(pinned, flag, 4, cudaMemcpyDeviceToHost, st));
+      sync();
+      wm = pinned[0] ? LV_WEIGHTS_FLOAT : LV_WEIGHTS_INTEGER;
+    }
+    wint = wm == LV_WEIGHTS_INTEGER;
+    setup_bins();
+    if (wint) configure_kernels<true>(); else configure_kernels<false>();
+    grid_n = ctx->sms * 8;
+    grid_sq = std::min(kMaxPartials, ctx->sms * 4);
+
+    LV_CUDA(cudaMemcpyAsync(D.col, col, (size_t)E * 4, kin, st));
+    long long* row64 = reinterpret_cast<long long*>(D.cd);  // (n+1) x 8 bytes, free until aggregation
+    LV_CUDA(cudaMemcpyAsync(row64, row_ptr, (size_t)(n + 1) * 8, kin, st));
+
+    // control block + graph states
+    LV_CUDA(cudaMemsetAsync(D.ctrl, 0, sizeof(Ctrl), st));
+    LV_CUDA(cudaMemsetAsync(D.gs, 0, sizeof(GraphState) * G, st));
+    Ctrl hc{};
+    std::memset(&hc, 0, offsetof(Ctrl, trace));
+    hc.it = 1;
+    hc.n = n; hc.E = E; hc.n0 = n0; hc.G = G;
+    hc.max_iterations = (uint32_t)std::max(0, cfg.max_iterations);
+    hc.threshold = cfg.threshold;
+    LV_CUDA(cudaMemcpyAsync(D.ctrl, &hc, offsetof(Ctrl, trace), cudaMemcpyHostToDevice, st));
+    std::vector<GraphState> hs(G);
+    std::vector<int64_t> ho(G + 1);
+    if (G > 1) {
+      LV_CUDA(cudaMemcpyAsync(ho.data(), offs, (G + 1) * sizeof(int64_t),
+                              in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, st));
+      sync();
+      if (ho[0] != 0 || ho[G] != n_) throw Fail{LV_ERR_ARGUMENT, "vtx_offsets must start at 0 and end at n"};
+      for (uint32_t g = 0; g < G; ++g)
+        if (ho[g + 1] <= ho[g]) throw Fail{LV_ERR_INPUT, "every graph of a batch needs at least one vertex"};
+    } else {
+      ho[0] = 0; ho[1] = n_;
+    }
+    for (uint32_t g = 0; g < G; ++g) {
+      std::memset(&hs[g], 0, sizeof(GraphState));
+      hs[g].vb = (uint32_t)ho[g];
+      hs[g].ve = (uint32_t)ho[g + 1];
+      hs[g].phase = kIterating;
+    }
+    LV_CUDA(cudaMemcpyAsync(D.gs, hs.data(), sizeof(GraphState) * G, cudaMemcpyHostToDevice, st));
+    if (G > 1) {
+      long long* doffs = dalloc<long long>(ctx, owned,(size_t)G + 1);
+      LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
+      k_fill_gid<<<std::min<uint32_t>(G, 65535), 256, 0, st>>>(D.gid, doffs, G);
+      LV_CUDA(cudaMemcpyAsync(D.gid0, D.gid, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    iota_best();
+    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
+    else k_prep<false><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
+    if (wint) k_prep_total<true><<<1, 256, 0, st>>>(D);
+    else k_prep_total<false><<<1, 256, 0, st>>>(D);
+    launches += 3 + (G > 1 ? 1 : 0) + (w && cfg.weight_mode == LV_WEIGHTS_AUTO ? 1 : 0);
+    check_device_errors();
+    level_start();
+  }
+
+  unsigned long long* scan_tmp = nullptr;
+  unsigned long long* scan_tot = nullptr;
+
+  void iota_best();
+
+  // ---- scans --------------------------------------------------------------------------------
+  template <class T, bool INCL>
+  void scan(const T* in, T* out, uint32_t count) {
+    if (count == 0) return;
+    const uint32_t tiles = (count + kScanTile - 1) / kScanTile;
+    T* tmp = reinterpret_cast<T*>(scan_tmp);
+    k_scan_tiles<T><<<tiles, kScanNT, 0, st>>>(in, tmp, count);
+    k_scan_sums<T><<<1, 1024, 0, st>>>(tmp, tiles);
+    k_scan_apply<T, INCL><<<tiles, kScanNT, 0, st>>>(in, out, tmp, count, nullptr);
+    launches += 3;
+  }
+
+  // ---- level start ------------------------------------------------------------------------------
+  void commit_sq() {
+    if (wint) k_commit_sq<true><<<grid_sq, 256, 0, st>>>(D, single() ? 1 : 0);
+    else k_commit_sq<false><<<grid_sq, 256, 0, st>>>(D, single() ? 1 : 0);
+  }
+  void finalize(int level_start_flag) {
+    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first);
+    else k_finalize<false><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first);
+  }
+
+  void ensure_arena(uint64_t need_slots) {
+    if (need_slots <= arena_slots) return;
+    if (need_slots >= 0xFFFFFFFFull) throw Fail{LV_ERR_RANGE, "hub hash-table arena beyond 2^32 slots"};
+    if (!arena_blocks.empty()) {
+      sync();
+      for (const Block& b : arena_blocks) ctx->give(b.p, b.bytes);
+      arena_blocks.clear();
+      D.arena_keys = nullptr;
+      D.arena_vals = nullptr;
+    }
+    uint64_t slots = std::max<uint64_t>(need_slots + need_slots / 4, 1 << 16);
+    slots = std::min<uint64_t>(slots, 0xFFFFFFFEull);
+    D.arena_keys = dalloc<uint32_t>(ctx, arena_blocks, slots);
+    D.arena_vals = dalloc<unsigned long long>(ctx, arena_blocks, slots);
+    arena_slots = slots;
+    write_ctrl_u32(offsetof(Ctrl, arena_slots), (uint32_t)slots);
+  }
+
+  void level_start() {
+    if (single() && cfg.chunk_edges > 0)
+      k_chunk_bounds<<<1, 1, 0, st>>>(D, (unsigned long long)cfg.chunk_edges);
+    k_level_init<<<grid_n, 256, 0, st>>>(D);
+    commit_sq();
+    finalize(1);
+    // global tables for the highest-degree vertices of this level
+    unsigned long long* need = scan_tot;
+    LV_CUDA(cudaMemsetAsync(need, 0, 8, st));
+    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], need);
+    launches += 4 + ((single() && cfg.chunk_edges > 0) ? 1 : 0);
+    LV_CUDA(cudaMemcpyAsync(pinned, need, 8, cudaMemcpyDeviceToHost, st));
+    sync();
+    uint64_t nd;
+    std::memcpy(&nd, pinned, 8);
+    ensure_arena(nd);
+    check_device_errors();
+  }
+
+  // ---- one optimisation pass --------------------------------------------------------------------
+  template <bool WI>
+  void launch_pass() {
+    const size_t slot = 4 + (WI ? 4 : 8);
+    LV_CUDA(cudaEventRecord(ev[4], st));
+    k_chunk_flags<<<grid_n, 256, 0, st>>>(D);
+    k_bin_vertices<<<grid_n, 256, 0, st>>>(D, bins);
+    k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
+    k_opt_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
+    k_opt_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
+    k_opt_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
+    k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
+    k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
+    k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
+    k_opt_block<WI, true><<<grid_block[1], 512, 0, st>>>(D, 7, 0);
+    LV_CUDA(cudaEventRecord(ev[5], st));
+    k_apply<WI><<<grid_n, 256, 0, st>>>(D);
+    commit_sq();
+    finalize(0);
+    launches += 13;
+  }
+
+  // Runs one pass; returns the number of graphs still iterating.
+  uint32_t pass() {
+    LV_CUDA(cudaEventRecord(ev[0], st));
+    if (wint) launch_pass<true>(); else launch_pass<false>();
+    LV_CUDA(cudaEventRecord(ev[1], st));
+    const uint32_t left = ctrl_u32(offsetof(Ctrl, n_iterating));
+    float ms = 0, mk = 0;
+    LV_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    LV_CUDA(cudaEventElapsedTime(&mk, ev[4], ev[5]));
+    t_opt_ms += ms;
+    t_optk_ms += mk;
+    return left;
+  }
+
+  void force_iterating() {
+    // phase-level API: an explicit pass on a graph whose level loop already stopped
+    const uint32_t it = kIterating;
+    LV_CUDA(cudaMemcpyAsync(&D.gs[0].phase, &it, 4, cudaMemcpyHostToDevice, st));
+  }
+
+  // ---- aggregation --------------------------------------------------------------------------------
+  // Returns true if any graph continues to a new level.
+  template <bool WI>
+  bool aggregate_impl(int force) {
+    const size_t slot = 4 + (WI ? 4 : 8);
+    k_agg_decide<<<std::max<uint32_t>(1, (G + 255) / 256), 256, 0, st>>>(D, force, (uint32_t)std::max(0, cfg.max_levels));
+    LV_CUDA(cudaMemsetAsync(D.map, 0, (size_t)n * 8, st));
+    k_agg_mark<<<grid_n, 256, 0, st>>>(D);
+    k_agg_flags<<<grid_n, 256, 0, st>>>(D);
+    scan<unsigned long long, true>(D.map, D.map, n);
+    k_agg_meta<<<std::max<uint32_t>(1, (G + 255) / 256), 256, 0, st>>>(D);
+    k_agg_best<<<grid_n, 256, 0, st>>>(D);
+    const uint32_t n2 = ctrl_u32(offsetof(Ctrl, n_next));
+    if (n2 > 0) {
+      LV_CUDA(cudaMemsetAsync(D.cd, 0, ((size_t)n2 + 1) * 8, st));
+      k_agg_count<<<grid_n, 256, 0, st>>>(D);
+      scan<unsigned long long, false>(D.cd, D.cd, n2 + 1);
+      k_agg_scatter<<<grid_n, 256, 0, st>>>(D);
+      k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
+      const uint32_t need = ctrl_u32(offsetof(Ctrl, hub_cursor));
+      ensure_arena(need);
+      k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
+      k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
+      k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
+      k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
+      k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
+      k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
+      k_contract_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
+      k_contract_block<WI, true><<<grid_block[1], 512, 0, st>>>(D, 7, 0);
+      LV_CUDA(cudaMemsetAsync(D.newdeg + n2, 0, 4, st));
+      scan<uint32_t, false>(D.newdeg, D.rowB, n2 + 1);
+      k_agg_compact<WI><<<grid_n, 256, 0, st>>>(D);
+      launches += 12;
+    }
+    k_agg_finish<<<grid_n, 256, 0, st>>>(D);
+    launches += 6;
+    check_device_errors();
+    n = ctrl_u32(offsetof(Ctrl, n));
+    E = ctrl_u32(offsetof(Ctrl, E));
+    return n2 > 0;
+  }
+
+  bool aggregate(int force) {
+    LV_CUDA(cudaEventRecord(ev[2], st));
+    const bool cont = wint ? aggregate_impl<true>(force) : aggregate_impl<false>(force);
+    LV_CUDA(cudaEventRecord(ev[3], st));
+    sync();
+    float ms = 0;
+    LV_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+    t_agg_ms += ms;
+    if (t_agg0 < 0) t_agg0 = ms;
+    ++levels_run;
+    if (cont) level_start();
+    else finished = true;
+    return cont;
+  }
+
+  // OptimizationPhase::run: passes until every graph of the batch has stopped its level.
+  int32_t optimization_run() {
+    int32_t passes = 0;
+    const double before = t_opt_ms;
+    while (true) {
+      ++passes;
+      if (pass() == 0) break;
+    }
+    if (t_opt0 < 0) t_opt0 = t_opt_ms - before;
+    check_device_errors();
+    return passes;
+  }
+
+  // modularity_routine's level loop.
+  void louvain() {
+    while (!finished) {
+      optimization_run();
+      aggregate(-1);
+    }
+  }
+
+  void stats(lv_stats* s) {
+    std::vector<GraphState> hs(G);
+    LV_CUDA(cudaMemcpyAsync(hs.data(), D.gs, sizeof(GraphState) * G, cudaMemcpyDeviceToHost, st));
+    sync();
+    unsigned long long act[2];
+    LV_CUDA(cudaMemcpyAsync(act, reinterpret_cast<char*>(D.ctrl) + offsetof(Ctrl, act_vertices_total),
+                            16, cudaMemcpyDeviceToHost, st));
+    sync();
+    std::memset(s, 0, sizeof(*s));
+    s->active_vertices = (int64_t)act[0];
+    s->active_entries = (int64_t)act[1];
+    // 12 B per active entry (destination, weight, destination's community) and 24 B per
+    // active vertex (row offsets, community, k, own total, decision)
+    s->bytes_optimization = 12.0 * (double)act[1] + 24.0 * (double)act[0];
+    s->ms_optimization_kernels = (float)t_optk_ms;
+    s->kernel_launches = launches;
+    s->modularity = hs[0].Q;
+    s->n = n0;
+    s->m = m_edges;
+    s->levels = levels_run;
+    s->iterations = (int32_t)hs[0].total_iters;
+    s->n_communities = (int32_t)hs[0].n_best;
+    s->ms_optimization = (float)t_opt_ms;
+    s->ms_aggregation = (float)t_agg_ms;
+    s->ms_first_optimization = (float)std::max(0.0, t_opt0);
+    s->ms_first_aggregation = (float)std::max(0.0, t_agg0);
+  }
+};
+
+__global__ void k_iota(uint32_t* p, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
+void Run::iota_best() { k_iota<<<grid_n ? grid_n : ctx->sms * 8, 256, 0, st>>>(D.best, n0); }
+
+}  // namespace lv
+
+struct lv_community {
+  lv_context* ctx;
+  std::unique_ptr<lv::Run> run;
+};
+
+// ---- C ABI --------------------------------------------------------------------------------------
+using lv::Fail;
+
+static lv_status fail(lv_context* ctx, const Fail& f) {
+  if (ctx) ctx->err = f.msg;
+  cudaGetLastError();  // clear a non-sticky launch error so the context stays usable
+  return f.st;
+}
+
+template <class F>
+static lv_status guarded(lv_context* ctx, F&& f) {
+  try {
+    f();
+    if (ctx) ctx->err.clear();
+    return LV_OK;
+  } catch (const Fail& e) {
+    return fail(ctx, e);
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, Fail{LV_ERR_NOMEM, "host allocation failed"});
+  } catch (...) {
+    return fail(ctx, Fail{LV_ERR_CUDA, "unexpected exception"});
+  }
+}
+
+extern "C" {
+
+int32_t lv_abi_version(void) { return 1; }
+
+const char* lv_status_string(lv_status s) {
+  const int i = (int)s;
+  return (i >= 0 && i <= 8) ? lv::kStatusText[i] : "unknown status";
+}
+
+void lv_config_default(lv_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->mode = LV_MODE_SORT;
+  c->fast_first = 1;
+  c->max_iterations = 1000000000;   // EARLY_STOP_LIMIT
+  c->max_levels = 0;
+  c->threshold = 0.001;             // MODULARITY_CONVERGED_THRESHOLD
+  c->chunk_edges = 50000000;        // STEP_ROUND
+  c->weight_mode = LV_WEIGHTS_AUTO;
+  c->validate = 1;
+  c->use_graphs = 1;
+}
+
+lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
+  if (!out) return LV_ERR_ARGUMENT;
+  *out = nullptr;
+  lv_context* ctx = new (std::nothrow) lv_context();
+  if (!ctx) return LV_ERR_NOMEM;
+  if (cfg) ctx->cfg = *cfg; else lv_config_default(&ctx->cfg);
+  if (ctx->cfg.mode < 0 || ctx->cfg.mode > 3 || !(ctx->cfg.threshold >= 0) ||
+      ctx->cfg.max_iterations < 0 || ctx->cfg.max_levels < 0 || ctx->cfg.chunk_edges < 0 ||
+      ctx->cfg.weight_mode < 0 || ctx->cfg.weight_mode > 2) {
+    delete ctx;
+    return LV_ERR_ARGUMENT;
+  }
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->pinned, 64);
+  for (auto& ev : ctx->ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  if (e != cudaSuccess) {
+    lv_destroy(ctx);
+    cudaGetLastError();
+    return LV_ERR_CUDA;
+  }
+  *out = ctx;
+  return LV_OK;
+}
+
+lv_status lv_destroy(lv_context* ctx) {
+  if (!ctx) return LV_ERR_ARGUMENT;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->drain_pool();
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LV_OK;
+}
+
+const char* lv_last_error(const lv_context* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+lv_status lv_community_create(lv_context* ctx, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                              const float* w, int32_t in_mem, lv_community** out) {
+  if (!ctx || !out) return LV_ERR_ARGUMENT;
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->device);
+    auto c = std::make_unique<lv_community>();
+    c->ctx = ctx;
+    c->run = std::make_unique<lv::Run>(ctx);
+    c->run->init(1, nullptr, n, row_ptr, col, w, in_mem);
+    *out = c.release();
+  });
+}
+
+lv_status lv_community_destroy(lv_community* c) {
+  if (!c) return LV_ERR_ARGUMENT;
+  delete c;
+  return LV_OK;
+}
+
+lv_status lv_optimization_step(lv_community* c, double* delta_q, int64_t* n_moved) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished (aggregation without contraction)"};
+    lv::GraphState before;
+    LV_CUDA(cudaMemcpy(&before, r.D.gs, sizeof(before), cudaMemcpyDeviceToHost));
+    r.force_iterating();
+    const uint32_t moved_before = r.ctrl_u32(offsetof(lv::Ctrl, trace_len));
+    r.pass();
+    r.check_device_errors();
+    lv::GraphState after;
+    LV_CUDA(cudaMemcpy(&after, r.D.gs, sizeof(after), cudaMemcpyDeviceToHost));
+    if (delta_q) *delta_q = after.Q - before.Q;
+    if (n_moved) *n_moved = after.moved;
+    (void)moved_before;
+  });
+}
+
+lv_status lv_optimization_run(lv_community* c, int32_t* iterations) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
+    r.force_iterating();
+    const int32_t it = r.optimization_run();
+    if (iterations) *iterations = it;
+  });
+}
+
+lv_status lv_aggregation_run(lv_community* c, int32_t aggregate) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
+    // the reference aggregates right after its optimisation loop; a graph still marked
+    // iterating (phase-level callers) takes part as if its level had stopped
+    const uint32_t done = lv::kLevelDone;
+    LV_CUDA(cudaMemcpyAsync(&r.D.gs[0].phase, &done, 4, cudaMemcpyHostToDevice, r.st));
+    r.aggregate(aggregate ? 1 : 0);
+  });
+}
+
+lv_status lv_louvain(lv_community* c, lv_stats* stats) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
+    r.louvain();
+    if (stats) r.stats(stats);
+  });
+}
+
+lv_status lv_community_info_get(lv_community* c, lv_community_info* info) {
+  if (!c || !info) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    lv::GraphState gs;
+    LV_CUDA(cudaMemcpyAsync(&gs, r.D.gs, sizeof(gs), cudaMemcpyDeviceToHost, r.st));
+    r.sync();
+    std::memset(info, 0, sizeof(*info));
+    info->n = r.finished ? 0 : r.n;
+    info->E = r.finished ? 0 : r.E;
+    info->n0 = r.n0;
+    info->level = (int32_t)gs.level;
+    info->iteration = (int32_t)gs.iters;
+    info->modularity = gs.Q;
+    info->internal = r.wint ? (double)gs.I : [&] { double d; std::memcpy(&d, &gs.I, 8); return d; }();
+    info->sum_a2 = r.wint ? (double)gs.S : [&] { double d; std::memcpy(&d, &gs.S, 8); return d; }();
+    info->total_weight = gs.m;
+    info->n_best = r.levels_run > 0 || r.finished ? gs.n_best : r.n0;
+    info->weights_integer = r.wint ? 1 : 0;
+  });
+}
+
+lv_status lv_community_get_partition(lv_community* c, int32_t* comm, double* totals) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished; use lv_community_get_best"};
+    if (comm) LV_CUDA(cudaMemcpyAsync(comm, r.D.comm, (size_t)r.n * 4, cudaMemcpyDeviceToHost, r.st));
+    if (totals) LV_CUDA(cudaMemcpyAsync(totals, r.D.a, (size_t)r.n * 8, cudaMemcpyDeviceToHost, r.st));
+    r.sync();
+  });
+}
+
+lv_status lv_community_get_best(lv_community* c, int32_t* best) {
+  if (!c || !best) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    LV_CUDA(cudaMemcpyAsync(best, r.D.best, (size_t)r.n0 * 4, cudaMemcpyDeviceToHost, r.st));
+    r.sync();
+  });
+}
+
+lv_status lv_community_get_graph(lv_community* c, int64_t* row_ptr, int32_t* col, double* w, double* k) {
+  if (!c) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
+    std::vector<uint32_t> hr(r.n + 1), hc(r.E), hw(r.E);
+    std::vector<double> hk(r.n);
+    LV_CUDA(cudaMemcpyAsync(hr.data(), r.D.row, (size_t)(r.n + 1) * 4, cudaMemcpyDeviceToHost, r.st));
+    LV_CUDA(cudaMemcpyAsync(hc.data(), r.D.col, (size_t)r.E * 4, cudaMemcpyDeviceToHost, r.st));
+    LV_CUDA(cudaMemcpyAsync(hw.data(), r.D.w, (size_t)r.E * 4, cudaMemcpyDeviceToHost, r.st));
+    LV_CUDA(cudaMemcpyAsync(hk.data(), r.D.k, (size_t)r.n * 8, cudaMemcpyDeviceToHost, r.st));
+    r.sync();
+    std::vector<std::pair<uint32_t, uint32_t>> rowbuf;
+    for (uint32_t v = 0; v < r.n; ++v) {
+      rowbuf.clear();
+      for (uint32_t e = hr[v]; e < hr[v + 1]; ++e) rowbuf.emplace_back(hc[e], hw[e]);
+      std::sort(rowbuf.begin(), rowbuf.end());
+      for (size_t i = 0; i < rowbuf.size(); ++i) {
+        const uint32_t e = hr[v] + (uint32_t)i;
+        if (col) col[e] = (int32_t)rowbuf[i].first;
+        if (w) {
+          if (r.wint) w[e] = (double)rowbuf[i].second;
+          else { float f; std::memcpy(&f, &rowbuf[i].second, 4); w[e] = (double)f; }
+        }
+      }
+    }
+    if (row_ptr)
+      for (uint32_t v = 0; v <= r.n; ++v) row_ptr[v] = hr[v];
+    if (k) std::memcpy(k, hk.data(), (size_t)r.n * 8);
+  });
+}
+
+lv_status lv_community_get_trace(lv_community* c, lv_trace_record* out, int32_t cap, int32_t* len) {
+  if (!c || !len || cap < 0 || (cap > 0 && !out)) return LV_ERR_ARGUMENT;
+  static_assert(sizeof(lv_trace_record) == sizeof(lv::TraceRec), "trace record layout");
+  std::lock_guard<std::mutex> lk(c->ctx->mu);
+  return guarded(c->ctx, [&] {
+    lv::Run& r = *c->run;
+    const uint32_t t = r.ctrl_u32(offsetof(lv::Ctrl, trace_len));
+    *len = (int32_t)t;
+    const uint32_t k = std::min<uint32_t>(t, (uint32_t)cap);
+    if (k) {
+      LV_CUDA(cudaMemcpyAsync(out, reinterpret_cast<char*>(r.D.ctrl) + offsetof(lv::Ctrl, trace),
+                              k * sizeof(lv::TraceRec), cudaMemcpyDeviceToHost, r.st));
+      r.sync();
+    }
+  });
+}
+
+static lv_status run_common(lv_context* ctx, uint32_t G, const int64_t* offs, int64_t n,
+                            const int64_t* row_ptr, const int32_t* col, const float* w, int32_t in_mem,
+                            int32_t* out_comm, int32_t out_mem, double* out_mod, int32_t* out_ncomm,
+                            lv_stats* stats) {
+  if (!ctx || !out_comm) return LV_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->device);
+    cudaEvent_t t0 = ctx->ev[0], t1 = ctx->ev[1], t2 = ctx->ev[2];
+    LV_CUDA(cudaEventRecord(t0, ctx->stream));
+    lv::Run r(ctx);
+    r.init(G, offs, n, row_ptr, col, w, in_mem);
+    LV_CUDA(cudaEventRecord(t1, ctx->stream));
+    r.louvain();
+    LV_CUDA(cudaMemcpyAsync(out_comm, r.D.out, (size_t)r.n0 * 4,
+                            out_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<lv::GraphState> hs(G);
+    LV_CUDA(cudaMemcpyAsync(hs.data(), r.D.gs, sizeof(lv::GraphState) * G, cudaMemcpyDeviceToHost, ctx->stream));
+    LV_CUDA(cudaEventRecord(t2, ctx->stream));
+    LV_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (out_mod) {
+      if (G == 1) *out_mod = hs[0].Q;
+      else for (uint32_t g = 0; g < G; ++g) out_mod[g] = hs[g].Q;
+    }
+    if (out_ncomm)
+      for (uint32_t g = 0; g < G; ++g) out_ncomm[g] = (int32_t)hs[g].n_best;
+    if (stats) {
+      r.stats(stats);
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, t0, t2);
+      cudaEventElapsedTime(&b, t1, t2);
+      stats->ms_total = a;
+      stats->ms_window = b;
+      stats->kernel_launches = r.launches;
+    }
+  });
+}
+
+lv_status lv_run_csr(lv_context* ctx, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                     const float* w, int32_t in_mem, int32_t* out_comm, int32_t out_mem,
+                     double* out_modularity, lv_stats* stats) {
+  return run_common(ctx, 1, nullptr, n, row_ptr, col, w, in_mem, out_comm, out_mem, out_modularity,
+                    nullptr, stats);
+}
+
+lv_status lv_run_batch(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offsets,
+                       const int64_t* row_ptr, const int32_t* col, const float* w, int32_t in_mem,
+                       int32_t* out_comm, int32_t out_mem, double* out_modularity, int32_t* out_ncomm,
+                       lv_stats* stats) {
+  if (!ctx || n_graphs <= 0 || !vtx_offsets) return LV_ERR_ARGUMENT;
+  int64_t n = 0;
+  if (in_mem == LV_MEM_DEVICE) {
+    if (cudaMemcpy(&n, vtx_offsets + n_graphs, 8, cudaMemcpyDeviceToHost) != cudaSuccess) return LV_ERR_CUDA;
+  } else {
+    n = vtx_offsets[n_graphs];
+  }
+  return run_common(ctx, (uint32_t)n_graphs, vtx_offsets, n, row_ptr, col, w, in_mem, out_comm, out_mem,
+                    out_modularity, out_ncomm, stats);
+}
+
+}  // extern "C"
+
+#include "lv_server.cuh"

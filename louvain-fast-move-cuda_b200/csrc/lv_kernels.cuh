@@ -1,0 +1,1198 @@
+// lv_kernels.cuh -- the engine's sm_100a kernels.
+//
+// One pass of the optimisation phase (the reference's optimize() + fast_move_update() +
+// compute_modularity(), phaseOptimization.cuh:116-181) is, here:
+//   k_chunk_flags -> k_bin_vertices -> k_opt_team<T> x6 / k_opt_block x2 -> k_apply ->
+//   k_commit_sq -> k_finalize
+// and aggregation (phaseAggregation.cuh:19-190) is:
+//   k_agg_flags -> scan -> k_agg_meta -> k_agg_best -> k_agg_count -> scan -> k_agg_scatter
+//   -> k_agg_bin -> k_contract_team<T> x6 / k_contract_block x2 -> scan -> k_agg_compact
+// All loops are grid-stride over sizes read from the device control block, so the grids do
+// not depend on the level and the sequence can be captured once and replayed.
+#pragma once
+
+#include "lv_device.cuh"
+
+namespace lv {
+
+// Everything a kernel needs about the current level. Pointers never change during a run
+// (aggregation copies the next level into the same buffers), so a captured launch stays
+// valid from level to level.
+struct Dev {
+  uint32_t* row;        // [n+1] edge offsets
+  uint32_t* col;        // [E] destination vertex
+  void* w;              // [E] u32 (integer mode) or f32 weights
+  double* k;            // [n] tot_weight_per_nodes
+  uint32_t* gid;        // [n] graph of each vertex (nullptr: one graph)
+  uint32_t* comm;       // [n] communities
+  double* a;            // [n] communities_weight
+  uint32_t* new_comm;   // [n] target of this pass's move
+  uint32_t* moved_it;   // [n] pass stamp of the last move
+  uint32_t* active_it;  // [n] pass stamp for which the vertex is active
+  uint32_t* bins[kNumBins];
+  uint32_t* hub_off;    // [n] arena offset per entry of the global-table bin
+  uint32_t* movers;     // [n]
+  uint32_t* arena_keys;
+  void* arena_vals;
+  GraphState* gs;
+  Ctrl* ctrl;
+  double* partials;     // [kMaxPartials] per-block partial sums (single graph)
+  // aggregation scratch
+  unsigned long long* map;   // [n] packed (nonempty, nonempty&&continue) inclusive counts
+  unsigned long long* cd;    // [n+1] packed (member count, degree sum) per new community
+  uint32_t* rank;            // [n] rank of a vertex inside its new community
+  uint32_t* members;         // [n]
+  uint32_t* newdeg;          // [n+1]
+  uint32_t* rowB;            // [n+1]
+  uint32_t* colB;            // [E]
+  void* wB;                  // [E]
+  double* kB;                // [n]
+  uint32_t* gidB;            // [n]
+  uint32_t* best;            // [n0] current-level vertex of each input vertex
+  uint32_t* gid0;            // [n0] graph of each input vertex (nullptr: one graph)
+  int32_t* out;              // [n0] final community ids
+};
+
+struct BinCfg {
+  uint32_t maxdeg[kNumBins];  // bin b: maxdeg[b-1] < d <= maxdeg[b]; the last bin is open
+};
+
+constexpr int kMaxPartials = 2048;
+
+__device__ __forceinline__ int bin_of(const BinCfg& B, uint32_t d) {
+#pragma unroll
+  for (int b = 0; b < kNumBins - 1; ++b)
+    if (d <= B.maxdeg[b]) return b;
+  return kNumBins - 1;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Append `item` to list `b` with one atomic per warp and bin. Every lane of the warp must
+// call it (bin == -1 for lanes with nothing to append). Returns the slot or kEmpty.
+__device__ __forceinline__ uint32_t warp_append(int bin, int b, uint32_t* counter) {
+  const unsigned mask = __ballot_sync(kFull, bin == b);
+  if (!mask) return kEmpty;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(kFull, base, leader);
+  return bin == b ? base + __popc(mask & lanemask_lt()) : kEmpty;
+}
+
+// Does vertex v take part in this pass at all: the reference's copy_if keeps edges with
+// changed[src] && src != dst (operatorsCommunity.h:7-19), so a vertex whose only entries are
+// self-loops selects nothing.
+__device__ __forceinline__ bool has_nonloop(const Dev& D, uint32_t v, uint32_t d) {
+  return d >= 2 || (d == 1 && D.col[D.row[v]] != v);
+}
+
+// ---- pass: chunk early-return emulation ---------------------------------------------------------
+// phaseOptimizationSort.cu:46-86 / 186-240 walk the edges in chunks of STEP_ROUND and
+// `return` from the whole pass at the first chunk whose copy_if selects nothing; vertices
+// of that chunk and of every later chunk are not considered in that pass.
+__global__ void k_chunk_flags(Dev D) {
+  Ctrl* C = D.ctrl;
+  if (!C->chunk_on || !(C->fast || C->rule_sort)) return;
+  const uint32_t n = C->n, it = C->it, nch = C->n_chunks;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    if (D.active_it[v] != it) continue;
+    const uint32_t d = D.row[v + 1] - D.row[v];
+    if (!has_nonloop(D, v, d)) continue;
+    uint32_t ch = 0;
+    while (ch + 1 < nch && C->chunk_lo[ch + 1] <= v) ++ch;
+    if (!((volatile uint32_t*)C->chunk_any)[ch]) atomicOr(&C->chunk_any[ch], 1u);
+  }
+}
+
+// ---- pass: degree binning of the active vertices ----------------------------------------------
+__global__ void k_bin_vertices(Dev D, BinCfg B) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n = C->n, it = C->it;
+  uint32_t v_end = n;
+  if (C->chunk_on && (C->fast || C->rule_sort)) {
+    for (uint32_t ch = 0; ch < C->n_chunks; ++ch)
+      if (!C->chunk_any[ch]) { v_end = C->chunk_lo[ch]; break; }
+  }
+  const bool want_off = !C->fast;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + threadIdx.x;
+    int bin = -1;
+    uint32_t d = 0;
+    if (v < v_end && D.active_it[v] == it) {
+      const uint32_t g = D.gid ? D.gid[v] : 0u;
+      if (D.gs[g].phase == kIterating) {
+        d = D.row[v + 1] - D.row[v];
+        if (d > 0) bin = bin_of(B, d);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kNumBins; ++b) {
+      const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
+      if (pos != kEmpty) {
+        D.bins[b][pos] = v;
+        if (b == kNumBins - 1 && want_off)
+          D.hub_off[pos] = atomicAdd(&C->hub_cursor, next_pow2(2u * d));
+      }
+    }
+    // pass accounting for the roofline: active vertices and their entries
+    const unsigned long long de = warp_sum((unsigned long long)(bin >= 0 ? d : 0u));
+    const unsigned nv = __popc(__ballot_sync(kFull, bin >= 0));
+    if ((threadIdx.x & 31) == 0 && nv) {
+      atomicAdd(&C->act_entries, de);
+      atomicAdd(&C->act_vertices, nv);
+    }
+  }
+}
+
+// Warp-aggregated append of movers; every lane of the warp must call it.
+__device__ __forceinline__ void emit_move(const Dev& D, bool move, uint32_t v, uint32_t c,
+                                          uint32_t it) {
+  const unsigned mask = __ballot_sync(kFull, move);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&D.ctrl->mover_count, (uint32_t)__popc(mask));
+  base = __shfl_sync(kFull, base, leader);
+  if (move) {
+    D.new_comm[v] = c;
+    D.moved_it[v] = it;
+    D.movers[base + __popc(mask & lanemask_lt())] = v;
+  }
+}
+
+struct VtxCtx {
+  uint32_t rs, re, cv;
+  double kv, a_own, m, two_m2;
+};
+
+__device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
+  VtxCtx x;
+  x.rs = D.row[v];
+  x.re = D.row[v + 1];
+  x.cv = D.comm[v];
+  x.kv = D.k[v];
+  x.a_own = D.a[x.cv];
+  const uint32_t g = D.gid ? D.gid[v] : 0u;
+  x.m = D.gs[g].m;
+  x.two_m2 = D.gs[g].two_m2;
+  return x;
+}
+
+// ---- pass: optimisation, one team of T lanes per vertex -----------------------------------------
+// Fast pass (iteration 0 of a level, phaseOptimizationSort.cu:28-158): per-entry gains with
+// self = 0 and the destination's own (singleton) community, argmax over positive gains with
+// the lowest community winning ties, then the v <= c gate (phaseOptimizationUpdate.cu:99).
+// Other passes (phaseOptimizationSort.cu:161-379 / phaseOptimizationHash.cu:38-162): exact
+// per-community sums of non-loop weights in a shared-memory hash table sized 2x the degree,
+// self_v = sum into the vertex's own community, gains for every other neighbouring
+// community, argmax with the mode's tie rule. Only positive gains can move a vertex, so only
+// they enter the argmax (the reference's own-community and negative candidates can never
+// win a move).
+template <int T, bool WINT>
+__global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  constexpr int TEAMS = 256 / T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int team = threadIdx.x / T, lane = threadIdx.x % T;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
+  Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
+
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[bin];
+  const uint32_t* list = D.bins[bin];
+  const uint32_t it = C->it;
+  const bool fast = C->fast != 0;
+  const bool lowest = fast || C->rule_sort != 0;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  uint32_t err = 0;
+
+  for (uint32_t base = blockIdx.x * TEAMS; base < count; base += gridDim.x * TEAMS) {
+    const uint32_t idx = base + team;
+    const bool live = idx < count;
+    const uint32_t v = live ? list[idx] : 0u;
+    VtxCtx x{};
+    if (live) x = load_vtx(D, v);
+    unsigned long long best = 0;
+    if (fast) {
+      if (live) {
+        for (uint32_t e = x.rs + lane; e < x.re; e += T) {
+          const uint32_t u = D.col[e];
+          if (u == v) continue;
+          const float g = gain_ref(Tr::w_float(w[e]), 0.0f, x.kv, x.a_own, D.a[u], x.m, x.two_m2);
+          if (g > 0.0f) {
+            const unsigned long long key = argmax_key(g, u, true);
+            best = key > best ? key : best;
+          }
+        }
+      }
+      best = team_max<T>(best, kFull);
+    } else {
+      const uint32_t cap_v = live ? next_pow2(2u * (x.re - x.rs)) : 2u;
+      const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+      if (live)
+        for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
+      __syncwarp();
+      if (live) {
+        for (uint32_t e = x.rs + lane; e < x.re; e += T) {
+          const uint32_t u = D.col[e];
+          if (u == v) continue;
+          if (!table_add(keys, vals, mask, shift, D.comm[u], (Acc)w[e])) err |= kErrTableFull;
+        }
+      }
+      __syncwarp();
+      if (live) {
+        const float self_v = Tr::to_float(table_get(keys, vals, mask, shift, x.cv));
+        for (uint32_t s = lane; s < cap_v; s += T) {
+          const uint32_t c = keys[s];
+          if (c == kEmpty || c == x.cv) continue;
+          const float g = gain_ref(Tr::to_float(vals[s]), self_v, x.kv, x.a_own, D.a[c], x.m, x.two_m2);
+          if (g > 0.0f) {
+            const unsigned long long key = argmax_key(g, c, lowest);
+            best = key > best ? key : best;
+          }
+        }
+      }
+      best = team_max<T>(best, kFull);
+      __syncwarp();
+    }
+    bool move = false;
+    uint32_t c = 0;
+    if (live && lane == 0 && best) {
+      c = key_comm(best, lowest);
+      move = c != x.cv && (!fast || v <= c);
+    }
+    emit_move(D, move, v, c, it);
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+// Block-wide max of a u64 (all threads call; result valid in every thread).
+template <int NT>
+__device__ __forceinline__ unsigned long long block_max(unsigned long long x, unsigned long long* sh) {
+  x = team_max<32>(x, kFull);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long y = lane < NT / 32 ? sh[lane] : 0ull;
+    y = team_max<32>(y, kFull);
+    if (lane == 0) sh[32] = y;
+  }
+  __syncthreads();
+  const unsigned long long r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+// ---- pass: optimisation, one block per high-degree vertex ----------------------------------------
+// GTABLE = false: the table lives in shared memory (capacity `cap` slots); true: the table is
+// a slice of the global arena at hub_off[idx] (vertices whose 2x degree exceeds shared
+// memory), touched through L2 atomics.
+template <bool WINT, bool GTABLE>
+__global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  constexpr int NT = 512;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned long long red[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[bin];
+  const uint32_t* list = D.bins[bin];
+  const uint32_t it = C->it;
+  const bool fast = C->fast != 0;
+  const bool lowest = fast || C->rule_sort != 0;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  uint32_t err = 0;
+
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const uint32_t v = list[idx];
+    const VtxCtx x = load_vtx(D, v);
+    unsigned long long best = 0;
+    if (fast) {
+      for (uint32_t e = x.rs + threadIdx.x; e < x.re; e += NT) {
+        const uint32_t u = D.col[e];
+        if (u == v) continue;
+        const float g = gain_ref(Tr::w_float(w[e]), 0.0f, x.kv, x.a_own, D.a[u], x.m, x.two_m2);
+        if (g > 0.0f) {
+          const unsigned long long key = argmax_key(g, u, true);
+          best = key > best ? key : best;
+        }
+      }
+    } else {
+      const uint32_t cap_v = next_pow2(2u * (x.re - x.rs));
+      const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+      uint32_t* keys;
+      Acc* vals;
+      bool ok = true;
+      if (GTABLE) {
+        const uint32_t off = D.hub_off[idx];
+        ok = (unsigned long long)off + cap_v <= C->arena_slots;
+        keys = D.arena_keys + off;
+        vals = reinterpret_cast<Acc*>(D.arena_vals) + off;
+      } else {
+        ok = cap_v <= cap;
+        keys = reinterpret_cast<uint32_t*>(smem);
+        vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
+      }
+      if (!ok) err |= kErrArena;
+      if (ok)
+        for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
+      __syncthreads();
+      if (ok) {
+        for (uint32_t e = x.rs + threadIdx.x; e < x.re; e += NT) {
+          const uint32_t u = D.col[e];
+          if (u == v) continue;
+          if (!table_add(keys, vals, mask, shift, D.comm[u], (Acc)w[e])) err |= kErrTableFull;
+        }
+      }
+      __syncthreads();
+      if (ok) {
+        const float self_v = Tr::to_float(table_get(keys, vals, mask, shift, x.cv));
+        for (uint32_t s = threadIdx.x; s < cap_v; s += NT) {
+          const uint32_t c = keys[s];
+          if (c == kEmpty || c == x.cv) continue;
+          const float g = gain_ref(Tr::to_float(vals[s]), self_v, x.kv, x.a_own, D.a[c], x.m, x.two_m2);
+          if (g > 0.0f) {
+            const unsigned long long key = argmax_key(g, c, lowest);
+            best = key > best ? key : best;
+          }
+        }
+      }
+    }
+    best = block_max<NT>(best, red);
+    if (threadIdx.x == 0 && best) {
+      const uint32_t c = key_comm(best, lowest);
+      if (c != x.cv && (!fast || v <= c)) {
+        D.new_comm[v] = c;
+        D.moved_it[v] = it;
+        D.movers[atomicAdd(&C->mover_count, 1u)] = v;
+      }
+    }
+    __syncthreads();
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+// ---- pass: apply the moves, propagate activity, update the internal weight ---------------------
+// update_value_kernel_* (phaseOptimizationUpdate.cu:14-115): totals of the old and new
+// community change by -/+ k_v with double atomics (integer-valued, so exact and
+// order-independent). update_changed_kernel (:117-132) -- "src is active next pass iff some
+// neighbour dst moved and comm[dst] != comm[src]" -- is evaluated by pushing from each mover
+// to its neighbours, which the symmetric CSR makes identical. The internal weight of
+// community.h:87-100 is kept incrementally: each directed entry (v,u) touching a mover
+// changes by w([post_v == post_u] - [pre_v == pre_u]); the mirror entry (u,v) is counted here
+// too when u did not move (factor 2).
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_apply(Dev D) {
+  using Tr = WTraits<WINT>;
+  using Wt = typename Tr::W;
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->mover_count, it = C->it;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t idx = warp; idx < count; idx += nwarps) {
+    const uint32_t v = D.movers[idx];
+    const uint32_t old = D.comm[v], nw = D.new_comm[v];
+    const double kv = D.k[v];
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (lane == 0) {
+      atomicAdd(&D.a[nw], kv);
+      atomicAdd(&D.a[old], -kv);
+    }
+    long long di = 0;
+    double df = 0.0;
+    const uint32_t rs = D.row[v], re = D.row[v + 1];
+    for (uint32_t e = rs + lane; e < re; e += 32) {
+      const uint32_t u = D.col[e];
+      const uint32_t pre = D.comm[u];
+      const bool mu = D.moved_it[u] == it;
+      const uint32_t post = mu ? D.new_comm[u] : pre;
+      if (post != nw) D.active_it[u] = it + 1;
+      const int dd = (int)(nw == post) - (int)(old == pre);
+      if (dd) {
+        const int f = mu ? dd : 2 * dd;
+        if (WINT) di += (long long)f * (long long)w[e];
+        else df += (double)f * Tr::w_double(w[e]);
+      }
+    }
+    if (WINT) {
+      di = warp_sum(di);
+      if (lane == 0 && di) atomicAdd(&D.gs[g].I, (unsigned long long)di);
+    } else {
+      df = warp_sum(df);
+      if (lane == 0 && df != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[g].I), df);
+    }
+  }
+}
+
+// ---- pass: commit moves and recompute sum_c a_c^2 -----------------------------------------------
+// Integer mode squares exactly in u64 (a_c <= 2m < 2^32). One graph: per-block partials,
+// summed in a fixed order by k_finalize. Several graphs: one block per graph.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_commit_sq(Dev D, int single) {
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->mover_count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t v = D.movers[i];
+    D.comm[v] = D.new_comm[v];
+  }
+  __shared__ double shd[33];
+  __shared__ unsigned long long shu[33];
+  if (single) {
+    const uint32_t n = C->n;
+    unsigned long long su = 0;
+    double sf = 0.0;
+    if (D.gs[0].phase == kIterating) {
+      for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const double x = D.a[c];
+        if (WINT) { const unsigned long long xi = (unsigned long long)x; su += xi * xi; }
+        else sf = __dadd_rn(sf, __dmul_rn(x, x));
+      }
+    }
+    if (WINT) {
+      unsigned long long tot;
+      block_excl_scan<unsigned long long, 256>(su, shu, &tot);
+      if (threadIdx.x == 0) reinterpret_cast<unsigned long long*>(D.partials)[blockIdx.x] = tot;
+    } else {
+      double tot;
+      block_excl_scan<double, 256>(sf, shd, &tot);
+      if (threadIdx.x == 0) D.partials[blockIdx.x] = tot;
+    }
+  } else {
+    for (uint32_t g = blockIdx.x; g < C->G; g += gridDim.x) {
+      GraphState* st = &D.gs[g];
+      if (st->phase != kIterating) continue;
+      unsigned long long su = 0;
+      double sf = 0.0;
+      for (uint32_t c = st->vb + threadIdx.x; c < st->ve; c += blockDim.x) {
+        const double x = D.a[c];
+        if (WINT) { const unsigned long long xi = (unsigned long long)x; su += xi * xi; }
+        else sf = __dadd_rn(sf, __dmul_rn(x, x));
+      }
+      if (WINT) {
+        unsigned long long tot;
+        block_excl_scan<unsigned long long, 256>(su, shu, &tot);
+        if (threadIdx.x == 0) st->S = tot;
+      } else {
+        double tot;
+        block_excl_scan<double, 256>(sf, shd, &tot);
+        if (threadIdx.x == 0) st->S = __double_as_longlong(tot);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double modularity_of(double I, double S, double m) {
+  // community.h:104: in / (2m) - sum_a2 / (4 m m)
+  return __dsub_rn(__ddiv_rn(I, __dmul_rn(2.0, m)), __ddiv_rn(S, __dmul_rn(__dmul_rn(4.0, m), m)));
+}
+
+// Sets ctrl->fast / rule_sort for pass index p of a level (execution_number in
+// phaseOptimization.cuh:116-146): p == 0 is the fast pass; afterwards SORT uses the lowest-c
+// rule, HASH / ADAPTIVE_MEMORY the highest-c rule, ADAPTIVE_SPEED the lowest-c rule for p <= 4.
+__device__ __forceinline__ void set_pass_rule(Ctrl* C, uint32_t p, int mode, int fast_first) {
+  C->fast = (fast_first && p == 0) ? 1u : 0u;
+  uint32_t sort_rule;
+  if (mode == 1) sort_rule = 1;
+  else if (mode == 2) sort_rule = p <= 4 ? 1u : 0u;
+  else sort_rule = 0;
+  C->rule_sort = sort_rule;
+}
+
+__global__ void k_set_pass(Ctrl* C, uint32_t p, int mode, int fast_first) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) set_pass_rule(C, p, mode, fast_first);
+}
+
+// ---- pass end: modularity, stop rule, counters ----------------------------------------------------
+// phaseOptimization.cuh:167-179: dQ = Q_after - Q_before; the level's passes stop when
+// dQ <= threshold (or after EARLY_STOP_LIMIT passes). `level_start` = 1 evaluates the level's
+// starting modularity instead (Community::update -> compute_modularity, community.h:57-65).
+template <bool WINT>
+__global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts, int level_start,
+                                                   int mode, int fast_first) {
+  Ctrl* C = D.ctrl;
+  __shared__ double shd[33];
+  __shared__ unsigned long long shu[33];
+  __shared__ uint32_t shc[33];
+  if (single) {
+    unsigned long long su = 0;
+    double sf = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+      if (WINT) su += reinterpret_cast<const unsigned long long*>(D.partials)[i];
+      else sf = __dadd_rn(sf, D.partials[i]);
+    }
+    if (WINT) {
+      unsigned long long tot;
+      block_excl_scan<unsigned long long, 1024>(su, shu, &tot);
+      if (threadIdx.x == 0 && D.gs[0].phase == kIterating) D.gs[0].S = tot;
+    } else {
+      double tot;
+      block_excl_scan<double, 1024>(sf, shd, &tot);
+      if (threadIdx.x == 0 && D.gs[0].phase == kIterating) D.gs[0].S = __double_as_longlong(tot);
+    }
+    __syncthreads();
+  }
+  uint32_t iterating = 0;
+  for (uint32_t g = threadIdx.x; g < C->G; g += blockDim.x) {
+    GraphState* st = &D.gs[g];
+    if (st->phase != kIterating) continue;
+    const double I = WINT ? (double)st->I : __longlong_as_double((long long)st->I);
+    const double S = WINT ? (double)st->S : __longlong_as_double((long long)st->S);
+    const double Q = modularity_of(I, S, st->m);
+    if (level_start) {
+      st->Q = Q;
+      st->Q_level = Q;
+      st->iters = 0;
+      ++iterating;
+      continue;
+    }
+    const double dq = __dsub_rn(Q, st->Q);
+    st->Q = Q;
+    st->iters += 1;
+    st->total_iters += 1;
+    if (single) {
+      st->moved = C->mover_count;
+      const uint32_t t = C->trace_len;
+      if (t < kTraceCap) {
+        TraceRec r;
+        r.level = st->level; r.iteration = st->iters - 1; r.n_moved = C->mover_count; r.pad = 0;
+        r.internal = I; r.sum_a2 = S; r.modularity = Q; r.delta = dq;
+        C->trace[t] = r;
+        C->trace_len = t + 1;
+      }
+    }
+    if (!(dq > C->threshold) || st->iters > C->max_iterations) st->phase = kLevelDone;
+    else ++iterating;
+  }
+  // count graphs still iterating
+  uint32_t tot;
+  block_excl_scan<uint32_t, 1024>(iterating, shc, &tot);
+  if (threadIdx.x == 0) {
+    C->n_iterating = tot;
+    C->loop_continue = tot > 0;
+    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    C->mover_count = 0;
+    C->hub_cursor = 0;
+    for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
+    C->act_entries_total += C->act_entries;
+    C->act_vertices_total += C->act_vertices;
+    C->act_entries = 0;
+    C->act_vertices = 0;
+    if (level_start) {
+      C->pass = 0;
+    } else {
+      C->it += 1;
+      C->pass += 1;
+    }
+    set_pass_rule(C, C->pass, mode, fast_first);
+  }
+}
+
+
+// ---- level start ------------------------------------------------------------------------------------
+// Community::update (community.h:57-65): identity partition, totals = k, every vertex active
+// (phaseOptimization.cuh:52).
+__global__ void k_level_init(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n = C->n, it = C->it;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (D.gs[g].phase != kIterating) continue;
+    D.comm[v] = v;
+    D.a[v] = D.k[v];
+    D.active_it[v] = it;
+    D.moved_it[v] = kNever;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C->mover_count = 0;
+    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    C->hub_cursor = 0;
+    for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
+  }
+}
+
+// Chunk bounds of the reference's edge loop for the current level (single graph):
+// limit = round + STEP; limit = (limit >= E) ? E : neighboorhood_sum[edge_source[limit] - 1].
+__global__ void k_chunk_bounds(Dev D, unsigned long long step) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctrl* C = D.ctrl;
+  const uint32_t n = C->n, E = C->E;
+  C->chunk_on = 0;
+  C->n_chunks = 1;
+  C->chunk_lo[0] = 0;
+  C->chunk_lo[1] = n;
+  if (step == 0 || (unsigned long long)E <= step) return;
+  unsigned long long round = 0;
+  uint32_t nch = 0;
+  while (round < E) {
+    if (nch >= kMaxChunks) { atomicOr(&C->err, kErrChunks); return; }
+    // first vertex of this chunk: the one whose row starts at `round`
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) { const uint32_t mid = (lo + hi) / 2; if (D.row[mid] <= round) lo = mid; else hi = mid; }
+    C->chunk_lo[nch++] = lo;
+    unsigned long long limit = round + step;
+    if (limit >= E) break;
+    lo = 0; hi = n;
+    while (hi - lo > 1) { const uint32_t mid = (lo + hi) / 2; if (D.row[mid] <= limit) lo = mid; else hi = mid; }
+    if (lo == 0) return;  // the reference would read neighboorhood_sum[-1]: no emulation
+    limit = D.row[lo - 1];
+    if (limit <= round) return;  // a row longer than STEP_ROUND: the reference loops forever; no emulation
+    round = limit;
+  }
+  C->n_chunks = nch;
+  C->chunk_lo[nch] = n;
+  C->chunk_on = 1;
+}
+
+// ---- level 0: input validation, weights, k, self-loop weight, total weight --------------------------
+// GraphDevice(GraphHost&) (graph.cuh:46-99) and the Community constructor (community.h:31-46):
+// k = sum of incident weights, m = total weight / 2 (graph.cu:81). One warp per vertex.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, const float* wf_in,
+                                              uint32_t n, unsigned long long E) {
+  Ctrl* C = D.ctrl;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t err = 0;
+  for (uint32_t v = warp; v < n; v += nwarps) {
+    const long long rs = row64[v], re = row64[v + 1];
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    const uint32_t lo = D.gs[g].vb, hi = D.gs[g].ve;
+    if (rs < 0 || re <= rs || (unsigned long long)re > E) {
+      if (lane == 0) { err |= kErrInput; D.row[v] = 0; D.k[v] = 0.0; }
+      continue;
+    }
+    if (lane == 0) {
+      D.row[v] = (uint32_t)rs;
+      if (v == n - 1) D.row[n] = (uint32_t)re;
+    }
+    unsigned long long ki = 0, si = 0;
+    double kf = 0.0, sf = 0.0;
+    for (long long e = rs + lane; e < re; e += 32) {
+      const uint32_t u = D.col[e];
+      if (u < lo || u >= hi) { err |= kErrInput; continue; }
+      const float x = wf_in ? wf_in[e] : 1.0f;
+      if (WINT) {
+        if (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f) { err |= kErrInput; continue; }
+        const uint32_t xi = (uint32_t)x;
+        reinterpret_cast<uint32_t*>(D.w)[e] = xi;
+        ki += xi;
+        if (u == v) si += xi;
+      } else {
+        if (!(x > 0.0f) || !(x < INFINITY)) { err |= kErrInput; continue; }
+        reinterpret_cast<float*>(D.w)[e] = x;
+        kf += (double)x;
+        if (u == v) sf += (double)x;
+      }
+    }
+    if (WINT) {
+      ki = warp_sum(ki);
+      si = warp_sum(si);
+      if (lane == 0) {
+        D.k[v] = (double)ki;
+        if (si) atomicAdd(&D.gs[g].I, si);
+        atomicAdd(&D.gs[g].S, ki);  // S temporarily holds sum k (= 2m) until k_prep_total
+      }
+    } else {
+      kf = warp_sum(kf);
+      sf = warp_sum(sf);
+      if (lane == 0) {
+        D.k[v] = kf;
+        if (sf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[g].I), sf);
+        atomicAdd(reinterpret_cast<double*>(&D.gs[g].S), kf);
+      }
+    }
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+// m = (sum of k) / 2 per graph; integer mode requires 2m < 2^32 (the reference's u32 sums).
+template <bool WINT>
+__global__ void k_prep_total(Dev D) {
+  Ctrl* C = D.ctrl;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
+    GraphState* st = &D.gs[g];
+    double twice;
+    if (WINT) {
+      if (st->S >= 4294967296ull) atomicOr(&C->err, kErrRange);
+      twice = (double)st->S;
+    } else {
+      twice = __longlong_as_double((long long)st->S);
+    }
+    st->m = twice / 2.0;
+    st->two_m2 = __dmul_rn(__dmul_rn(2.0, st->m), st->m);
+    st->S = 0;
+  }
+}
+
+// Integer-weight detection for LV_WEIGHTS_AUTO: any weight that is not a non-negative integer
+// representable in u32 selects float mode.
+__global__ void k_weights_integral(const float* w, unsigned long long E, uint32_t* flag) {
+  for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < E;
+       e += (unsigned long long)gridDim.x * blockDim.x) {
+    const float x = w[e];
+    if (!(x >= 0.0f) || x != floorf(x) || x > 4294967040.0f) { *flag = 1; return; }
+  }
+}
+
+// Graph ids of each vertex from the packed offsets (batched input).
+__global__ void k_fill_gid(uint32_t* gid, const long long* offs, uint32_t G) {
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
+    const long long b = offs[g], e = offs[g + 1];
+    for (long long v = b + threadIdx.x; v < e; v += blockDim.x) gid[v] = g;
+  }
+}
+
+// Hash-table arena needed by the global-table bin at this level: sum over vertices with
+// degree above the shared-memory bound of next_pow2(2 d).
+__global__ void k_arena_need(Dev D, uint32_t min_deg, unsigned long long* need) {
+  const uint32_t n = D.ctrl->n;
+  unsigned long long s = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t d = D.row[v + 1] - D.row[v];
+    if (d > min_deg) s += next_pow2(2u * d);
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(need, s);
+}
+
+// ---- aggregation -------------------------------------------------------------------------------------
+// phaseAggregation.cuh:27-43: new id = inclusive count of nonempty communities minus one. The
+// reference tests a_c > 0 (CountNotZero); with every weight positive that is exactly "has a
+// member", which is what is marked here, so no rounding residue in a_c can create an empty
+// row. The low word counts only communities of graphs that continue to a new level.
+__global__ void k_agg_mark(Dev D) {
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    D.map[D.comm[v]] = 1ull;
+}
+
+__global__ void k_agg_flags(Dev D) {
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const uint32_t g = D.gid ? D.gid[c] : 0u;
+    const unsigned long long ne = D.map[c] != 0ull ? 1ull : 0ull;
+    D.map[c] = (ne << 32) | (ne & (unsigned long long)D.gs[g].cont);
+  }
+}
+
+// Per graph: n_of_best_communities, base of its final ids, next-level vertex range.
+__global__ void k_agg_meta(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n = C->n;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
+    GraphState* st = &D.gs[g];
+    if (!st->agg) continue;
+    const unsigned long long before = st->vb > 0 ? D.map[st->vb - 1] : 0ull;
+    const unsigned long long end = D.map[st->ve - 1];
+    st->map_base = (uint32_t)(before >> 32);
+    st->n_best = (uint32_t)(end >> 32) - st->map_base;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) C->n_next = n ? (uint32_t)D.map[n - 1] : 0u;
+}
+
+// community.h:48-55 update_best: best[v0] = new(comm[best[v0]]). Graphs that stop here get
+// their final ids (0..K-1 within the graph) written to `out`.
+__global__ void k_agg_best(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n0 = C->n0;
+  for (uint32_t v0 = blockIdx.x * blockDim.x + threadIdx.x; v0 < n0; v0 += gridDim.x * blockDim.x) {
+    const uint32_t g = D.gid0 ? D.gid0[v0] : 0u;
+    const GraphState& st = D.gs[g];
+    if (!st.agg) continue;
+    const uint32_t b = D.best[v0];
+    const unsigned long long mv = D.map[D.comm[b]];
+    if (st.cont) {
+      D.best[v0] = (uint32_t)mv - 1u;
+    } else {
+      const uint32_t id = (uint32_t)(mv >> 32) - 1u - st.map_base;
+      D.best[v0] = id;
+      D.out[v0] = (int32_t)id;
+    }
+  }
+}
+
+// Count members and degree sums of each new community (packed, one atomic per vertex); the
+// returned old value is the vertex's rank inside its community.
+__global__ void k_agg_count(Dev D) {
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (!D.gs[g].cont) continue;
+    const uint32_t s = (uint32_t)D.map[D.comm[v]] - 1u;
+    const uint32_t d = D.row[v + 1] - D.row[v];
+    const unsigned long long old = atomicAdd(&D.cd[s], (1ull << 32) | d);
+    D.rank[v] = (uint32_t)(old >> 32);
+    D.new_comm[v] = s;  // next-level id of v's community, read by the contraction
+  }
+}
+
+__global__ void k_agg_scatter(Dev D) {
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (!D.gs[g].cont) continue;
+    const uint32_t s = D.new_comm[v];
+    D.members[(uint32_t)(D.cd[s] >> 32) + D.rank[v]] = v;
+  }
+}
+
+// Bin the new communities by their summed member degree (the contraction's work).
+__global__ void k_agg_bin(Dev D, BinCfg B) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n2 = C->n_next;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n2; base += gridDim.x * blockDim.x) {
+    const uint32_t s = base + threadIdx.x;
+    int bin = -1;
+    uint32_t dsum = 0;
+    if (s < n2) {
+      dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
+      bin = bin_of(B, dsum);
+    }
+#pragma unroll
+    for (int b = 0; b < kNumBins; ++b) {
+      const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
+      if (pos != kEmpty) {
+        D.bins[b][pos] = s;
+        if (b == kNumBins - 1) D.hub_off[pos] = atomicAdd(&C->hub_cursor, next_pow2(2u * dsum));
+      }
+    }
+  }
+}
+
+struct CommCtx {
+  uint32_t mb, me, tb, dsum, g;
+};
+
+__device__ __forceinline__ CommCtx load_comm(const Dev& D, uint32_t s) {
+  CommCtx x;
+  const unsigned long long a = D.cd[s], b = D.cd[s + 1];
+  x.mb = (uint32_t)(a >> 32);
+  x.me = (uint32_t)(b >> 32);
+  x.tb = (uint32_t)a;
+  x.dsum = (uint32_t)b - (uint32_t)a;
+  const uint32_t v0 = D.members[x.mb];
+  x.g = D.gid ? D.gid[v0] : 0u;
+  return x;
+}
+
+// Contraction of one new community s (phaseAggregation.cuh:51-106 for SORT,
+// :107-141 for HASH): every entry (v,u,w) of every member v goes to (s, new(comm u)), weights
+// summed exactly (u32 in integer mode, double then one fp32 rounding in float mode). The
+// unique destinations are written to colB/wB at the community's degree-sum offset, the row
+// length to newdeg, k' = row sum to kB, the self-loop weight to the graph's next-level I.
+template <int T, bool WINT>
+__global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t cap) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  constexpr int TEAMS = 256 / T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int team = threadIdx.x / T, lane = threadIdx.x % T;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
+  Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[bin];
+  const uint32_t* list = D.bins[bin];
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
+  uint32_t err = 0;
+  for (uint32_t base = blockIdx.x * TEAMS; base < count; base += gridDim.x * TEAMS) {
+    const uint32_t idx = base + team;
+    const bool live = idx < count;
+    const uint32_t s = live ? list[idx] : 0u;
+    CommCtx x{};
+    if (live) x = load_comm(D, s);
+    const uint32_t cap_v = live ? next_pow2(2u * (x.dsum > 0 ? x.dsum : 1u)) : 2u;
+    const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+    if (live)
+      for (uint32_t i = lane; i < cap_v; i += T) { keys[i] = kEmpty; vals[i] = Acc(0); }
+    __syncwarp();
+    if (live) {
+      for (uint32_t i = x.mb; i < x.me; ++i) {
+        const uint32_t v = D.members[i];
+        const uint32_t re = D.row[v + 1];
+        for (uint32_t e = D.row[v] + lane; e < re; e += T) {
+          const uint32_t d = D.new_comm[D.col[e]];
+          if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+        }
+      }
+    }
+    __syncwarp();
+    // compact the occupied slots of this team's table into the output row
+    uint32_t cnt = 0;
+    double ksum = 0.0;
+    if (live)
+      for (uint32_t i = lane; i < cap_v; i += T) cnt += keys[i] != kEmpty;
+    uint32_t off = cnt;
+#pragma unroll
+    for (int o = 1; o < T; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, off, o, T);
+      if (lane >= o) off += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, off, T - 1, T);
+    off -= cnt;
+    if (live) {
+      for (uint32_t i = lane; i < cap_v; i += T) {
+        const uint32_t d = keys[i];
+        if (d == kEmpty) continue;
+        const Acc sum = vals[i];
+        Wt wv;
+        if (WINT) wv = (Wt)sum;
+        else wv = (Wt)__double2float_rn((double)sum);
+        D.colB[x.tb + off] = d;
+        wout[x.tb + off] = wv;
+        ++off;
+        ksum += Tr::w_double(wv);
+        if (d == s) {
+          if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
+          else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), (double)wv);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) ksum += __shfl_xor_sync(kFull, ksum, o, T);
+    if (live && lane == 0) {
+      D.newdeg[s] = total;
+      D.kB[s] = ksum;
+      if (D.gidB) D.gidB[s] = x.g;
+    }
+    __syncwarp();
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+template <bool WINT, bool GTABLE>
+__global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t cap) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  constexpr int NT = 512;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t shu[33];
+  __shared__ double shd[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[bin];
+  const uint32_t* list = D.bins[bin];
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
+  uint32_t err = 0;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const uint32_t s = list[idx];
+    const CommCtx x = load_comm(D, s);
+    const uint32_t cap_v = next_pow2(2u * (x.dsum > 0 ? x.dsum : 1u));
+    const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+    uint32_t* keys;
+    Acc* vals;
+    bool ok;
+    if (GTABLE) {
+      const uint32_t off = D.hub_off[idx];
+      ok = (unsigned long long)off + cap_v <= C->arena_slots;
+      keys = D.arena_keys + off;
+      vals = reinterpret_cast<Acc*>(D.arena_vals) + off;
+    } else {
+      ok = cap_v <= cap;
+      keys = reinterpret_cast<uint32_t*>(smem);
+      vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
+    }
+    if (!ok) err |= kErrArena;
+    if (ok)
+      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) { keys[i] = kEmpty; vals[i] = Acc(0); }
+    __syncthreads();
+    if (ok) {
+      // members with small rows: one member per warp lane group; long rows: whole block
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      for (uint32_t i = x.mb + wid; i < x.me; i += NT / 32) {
+        const uint32_t v = D.members[i];
+        const uint32_t re = D.row[v + 1];
+        for (uint32_t e = D.row[v] + lane; e < re; e += 32) {
+          const uint32_t d = D.new_comm[D.col[e]];
+          if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t cnt = 0;
+    if (ok)
+      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) cnt += keys[i] != kEmpty;
+    uint32_t total;
+    uint32_t off = block_excl_scan<uint32_t, NT>(cnt, shu, &total);
+    double ksum = 0.0;
+    if (ok) {
+      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) {
+        const uint32_t d = keys[i];
+        if (d == kEmpty) continue;
+        const Acc sum = vals[i];
+        Wt wv;
+        if (WINT) wv = (Wt)sum;
+        else wv = (Wt)__double2float_rn((double)sum);
+        D.colB[x.tb + off] = d;
+        wout[x.tb + off] = wv;
+        ++off;
+        ksum += Tr::w_double(wv);
+        if (d == s) {
+          if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
+          else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), (double)wv);
+        }
+      }
+    }
+    double ktot;
+    block_excl_scan<double, NT>(ksum, shd, &ktot);
+    if (threadIdx.x == 0) {
+      D.newdeg[s] = ok ? total : 0u;
+      D.kB[s] = ktot;
+      if (D.gidB) D.gidB[s] = x.g;
+    }
+    __syncthreads();
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+// Copy the gapped contracted rows into the dense next-level CSR (col/w), move k' and gid'.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_agg_compact(Dev D) {
+  using Wt = typename WTraits<WINT>::W;
+  Ctrl* C = D.ctrl;
+  const uint32_t n2 = C->n_next;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const Wt* __restrict__ win = reinterpret_cast<const Wt*>(D.wB);
+  Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.w);
+  for (uint32_t s = warp; s < n2; s += nwarps) {
+    const uint32_t src = (uint32_t)D.cd[s], dst = D.rowB[s], len = D.rowB[s + 1] - dst;
+    for (uint32_t i = lane; i < len; i += 32) {
+      D.col[dst + i] = D.colB[src + i];
+      wout[dst + i] = win[src + i];
+    }
+    if (lane == 0) {
+      D.k[s] = D.kB[s];
+      if (D.gid) D.gid[s] = D.gidB[s];
+    }
+  }
+}
+
+__global__ void k_agg_finish(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n2 = C->n_next;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s <= n2; s += gridDim.x * blockDim.x)
+    D.row[s] = D.rowB[s];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C->E_next = D.rowB[n2];
+    // per-graph next-level ranges (graphs keep their order; finished graphs drop out)
+    for (uint32_t g = 0; g < C->G; ++g) {
+      GraphState* st = &D.gs[g];
+      if (!st->agg) continue;
+      if (st->cont) {
+        const uint32_t before = st->vb > 0 ? (uint32_t)D.map[st->vb - 1] : 0u;
+        const uint32_t end = (uint32_t)D.map[st->ve - 1];
+        st->vb = before;
+        st->ve = end;
+        st->level += 1;
+        st->phase = kIterating;
+      } else {
+        st->phase = kFinished;
+        st->vb = st->ve = 0;
+      }
+      st->agg = 0;
+    }
+    C->n = n2;
+    C->E = C->E_next;
+  }
+}
+
+// Which graphs aggregate now and whether they continue: modularityAlgorithms.h:52
+// cont = Q_end - Q_level_start > threshold. force >= 0 overrides (phase-level API).
+__global__ void k_agg_decide(Dev D, int force, uint32_t max_levels) {
+  Ctrl* C = D.ctrl;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
+    GraphState* st = &D.gs[g];
+    if (st->phase == kFinished) { st->agg = 0; continue; }
+    st->agg = 1;
+    uint32_t cont;
+    if (force >= 0) cont = (uint32_t)force;
+    else cont = __dsub_rn(st->Q, st->Q_level) > C->threshold ? 1u : 0u;
+    if (max_levels > 0 && st->level + 1 >= max_levels) cont = 0;
+    st->cont = cont;
+    if (cont) st->I = 0;  // the contraction adds the next level's self-loop weight
+  }
+}
+
+// ---- scans (3-phase: tile sums, scan of tile sums, tile scan + offset) ---------------------------
+constexpr int kScanNT = 256;
+constexpr int kScanIPT = 8;
+constexpr int kScanTile = kScanNT * kScanIPT;
+
+template <class T>
+__global__ void __launch_bounds__(kScanNT) k_scan_tiles(const T* in, T* tile_sums, uint32_t n) {
+  __shared__ T sh[33];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < kScanIPT; ++i) {
+    const uint64_t j = base + (uint64_t)i * kScanNT + threadIdx.x;
+    if (j < n) s += in[j];
+  }
+  T tot;
+  block_excl_scan<T, kScanNT>(s, sh, &tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntiles) {
+  __shared__ T sh[33];
+  // each thread scans a contiguous run, then the block scans the run totals
+  const uint32_t per = (ntiles + 1023) / 1024;
+  const uint32_t b = threadIdx.x * per, e = min(b + per, ntiles);
+  T s = T(0);
+  for (uint32_t i = b; i < e; ++i) s += tile_sums[i];
+  T tot;
+  T off = block_excl_scan<T, 1024>(s, sh, &tot);
+  for (uint32_t i = b; i < e; ++i) {
+    const T x = tile_sums[i];
+    tile_sums[i] = off;
+    off += x;
+  }
+}
+
+// inclusive = true: out[i] = sum in[0..i]; false: out[i] = sum in[0..i-1], and if
+// total_out != nullptr the grand total is written there.
+template <class T, bool INCLUSIVE>
+__global__ void __launch_bounds__(kScanNT) k_scan_apply(const T* in, T* out, const T* tile_offs,
+                                                         uint32_t n, T* total_out) {
+  __shared__ T sh[33];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanIPT;
+  T vals[kScanIPT];
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < kScanIPT; ++i) {
+    const uint64_t j = base + i;
+    vals[i] = j < n ? in[j] : T(0);
+    s += vals[i];
+  }
+  T tot;
+  T run = block_excl_scan<T, kScanNT>(s, sh, &tot) + tile_offs[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanIPT; ++i) {
+    const uint64_t j = base + i;
+    if (INCLUSIVE) run += vals[i];
+    if (j < n) out[j] = run;
+    if (!INCLUSIVE) run += vals[i];
+  }
+  if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == kScanNT - 1) *total_out = run;
+}
+
+}  // namespace lv

@@ -325,7 +325,10 @@ static int has_selected_edge(const orc_state* s, int64_t v) {
 static int64_t optimization_step(orc_state* s) {
     int64_t n = s->n;
     const int fast = s->cfg.fast_first && s->iter_in_level == 0;
-    const int hash_rule = (s->cfg.mode == 0) && !fast;
+    /* phaseOptimization.cuh:135: HASH and ADAPTIVE_MEMORY use the hash rule from pass 1,
+     * ADAPTIVE_SPEED after pass 4 */
+    const int m_ = s->cfg.mode;
+    const int hash_rule = !fast && (m_ == 0 || m_ == 3 || (m_ == 2 && s->iter_in_level > 4));
     /* which vertices does this pass consider (chunk early return) */
     int64_t v_end = n;
     int chunk_rule = (s->cfg.chunk_edges > 0) && (fast || !hash_rule);
