@@ -47,8 +47,18 @@ struct GraphState {
   uint32_t map_base;  // aggregation: nonempty communities before this graph
   uint32_t total_iters;
   uint32_t moved;     // moves of the last pass
-  uint32_t pad;
+  uint32_t n_next;    // aggregation: vertices of this graph at the next level
 };
+
+// Hash-table capacity for a row of d entries in a graph of ng vertices: twice the number of
+// distinct keys it can hold (at most min(d, ng)), rounded up to a power of two.
+__host__ __device__ __forceinline__ uint32_t table_cap(uint32_t d, uint32_t ng) {
+  uint32_t k = d < ng ? d : ng;
+  if (k < 1) k = 1;
+  uint32_t p = 2;
+  while (p < 2u * k) p <<= 1;
+  return p;
+}
 
 struct TraceRec {
   uint32_t level, iteration, n_moved, pad;
@@ -67,7 +77,8 @@ struct Ctrl {
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
   uint32_t bin_count[kNumBins];
-  uint32_t mover_count;
+  uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
+  uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
   uint32_t hub_cursor;         // global hash-table arena cursor (slots)
   uint32_t arena_slots;        // arena capacity (slots)
   uint32_t n_next, E_next;     // aggregation outputs

@@ -203,6 +203,7 @@ class Run {
     for (int b = 0; b < kNumBins; ++b)
       bins.maxdeg[b] = cfg.bin_max_degree[b] > 0 ? (uint32_t)cfg.bin_max_degree[b] : kDefaultMaxDeg[b];
     bins.maxdeg[kNumBins - 1] = 0xFFFFFFFFu;
+    bins.block_cap = next_pow2(2u * std::max(1u, bins.maxdeg[6]));
     for (int b = 0; b + 1 < kNumBins; ++b)
       if (bins.maxdeg[b + 1] < bins.maxdeg[b]) throw Fail{LV_ERR_ARGUMENT, "bin_max_degree must be non-decreasing"};
     for (int b = 0; b < 6; ++b) team_cap[b] = next_pow2(2u * std::max(1u, bins.maxdeg[b]));
@@ -237,7 +238,7 @@ class Run {
     team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     const size_t bsmem = (size_t)block_cap * (4 + acc_size());
     LV_CUDA(cudaFuncSetAttribute((const void*)k_opt_block<WI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
-    LV_CUDA(cudaFuncSetAttribute((const void*)k_contract_block<WI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    LV_CUDA(cudaFuncSetAttribute((const void*)k_contract_block<WI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
     int occ = 0;
     LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, false>, 512, bsmem));
     grid_block[0] = ctx->sms * std::max(1, occ);
@@ -281,6 +282,7 @@ class Run {
     D.active_it = dalloc<uint32_t>(ctx, owned,n);
     for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned,n);
     D.hub_off = dalloc<uint32_t>(ctx, owned,n);
+    D.hubtab = dalloc<uint32_t>(ctx, owned, n);
     D.movers = dalloc<uint32_t>(ctx, owned,n);
     D.gs = dalloc<GraphState>(ctx, owned,G);
     D.ctrl = dalloc<Ctrl>(ctx, owned,1);
@@ -412,6 +414,7 @@ class Run {
     slots = std::min<uint64_t>(slots, 0xFFFFFFFEull);
     D.arena_keys = dalloc<uint32_t>(ctx, arena_blocks, slots);
     D.arena_vals = dalloc<unsigned long long>(ctx, arena_blocks, slots);
+    D.hub_owner = dalloc<uint32_t>(ctx, arena_blocks, slots / kHubChunk + 1);
     arena_slots = slots;
     write_ctrl_u32(offsetof(Ctrl, arena_slots), (uint32_t)slots);
   }
@@ -425,7 +428,7 @@ class Run {
     // global tables for the highest-degree vertices of this level
     unsigned long long* need = scan_tot;
     LV_CUDA(cudaMemsetAsync(need, 0, 8, st));
-    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], need);
+    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], bins.block_cap, need);
     launches += 4 + ((single() && cfg.chunk_edges > 0) ? 1 : 0);
     LV_CUDA(cudaMemcpyAsync(pinned, need, 8, cudaMemcpyDeviceToHost, st));
     sync();
@@ -452,9 +455,10 @@ class Run {
     k_opt_block<WI, true><<<grid_block[1], 512, 0, st>>>(D, 7, 0);
     LV_CUDA(cudaEventRecord(ev[5], st));
     k_apply<WI><<<grid_n, 256, 0, st>>>(D);
+    k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(D);
     commit_sq();
     finalize(0);
-    launches += 13;
+    launches += 14;
   }
 
   // Runs one pass; returns the number of graphs still iterating.
@@ -495,21 +499,30 @@ class Run {
       k_agg_count<<<grid_n, 256, 0, st>>>(D);
       scan<unsigned long long, false>(D.cd, D.cd, n2 + 1);
       k_agg_scatter<<<grid_n, 256, 0, st>>>(D);
+      LV_CUDA(cudaMemsetAsync(D.hubtab, 0xFF, (size_t)n2 * 4, st));
       k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
       const uint32_t need = ctrl_u32(offsetof(Ctrl, hub_cursor));
       ensure_arena(need);
+      if (need > 0) {
+        // the largest new communities: many blocks insert into their global tables
+        LV_CUDA(cudaMemsetAsync(D.arena_keys, 0xFF, (size_t)need * 4, st));
+        LV_CUDA(cudaMemsetAsync(D.arena_vals, 0, (size_t)need * 8, st));
+        k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(D, kNumBins - 1);
+        k_hub_insert<WI><<<grid_n, 256, 0, st>>>(D);
+        k_hub_emit<WI><<<std::min<uint32_t>(need / kHubChunk, (uint32_t)ctx->sms * 8), 512, 0, st>>>(D, need / kHubChunk);
+        launches += 3;
+      }
       k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
       k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
       k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
       k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
       k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
       k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
-      k_contract_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
-      k_contract_block<WI, true><<<grid_block[1], 512, 0, st>>>(D, 7, 0);
+      k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
       LV_CUDA(cudaMemsetAsync(D.newdeg + n2, 0, 4, st));
       scan<uint32_t, false>(D.newdeg, D.rowB, n2 + 1);
       k_agg_compact<WI><<<grid_n, 256, 0, st>>>(D);
-      launches += 12;
+      launches += 11;
     }
     k_agg_finish<<<grid_n, 256, 0, st>>>(D);
     launches += 6;

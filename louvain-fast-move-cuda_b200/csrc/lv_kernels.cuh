@@ -31,9 +31,11 @@ struct Dev {
   uint32_t* active_it;  // [n] pass stamp for which the vertex is active
   uint32_t* bins[kNumBins];
   uint32_t* hub_off;    // [n] arena offset per entry of the global-table bin
+  uint32_t* hubtab;     // [n] aggregation: arena offset of each bin-7 new community, else kEmpty
   uint32_t* movers;     // [n]
   uint32_t* arena_keys;
-  void* arena_vals;
+  void* arena_vals;     // 8 bytes per slot
+  uint32_t* hub_owner;  // [arena slots / kHubChunk] new community owning each table chunk
   GraphState* gs;
   Ctrl* ctrl;
   double* partials;     // [kMaxPartials] per-block partial sums (single graph)
@@ -55,7 +57,11 @@ struct Dev {
 
 struct BinCfg {
   uint32_t maxdeg[kNumBins];  // bin b: maxdeg[b-1] < d <= maxdeg[b]; the last bin is open
+  uint32_t block_cap;         // shared-memory table slots of the block kernels (bin 6)
 };
+
+// Table granule of the multi-block global tables: every global table is a multiple of it.
+constexpr uint32_t kHubChunk = 4096;
 
 constexpr int kMaxPartials = 2048;
 
@@ -123,12 +129,19 @@ __global__ void k_bin_vertices(Dev D, BinCfg B) {
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const uint32_t v = base + threadIdx.x;
     int bin = -1;
-    uint32_t d = 0;
+    uint32_t d = 0, cap = 0;
     if (v < v_end && D.active_it[v] == it) {
       const uint32_t g = D.gid ? D.gid[v] : 0u;
       if (D.gs[g].phase == kIterating) {
         d = D.row[v + 1] - D.row[v];
-        if (d > 0) bin = bin_of(B, d);
+        if (d > 0) {
+          bin = bin_of(B, d);
+          // a long row whose distinct communities fit the shared table stays in bin 6
+          if (bin == kNumBins - 1) {
+            cap = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
+            if (cap <= B.block_cap) bin = kNumBins - 2;
+          }
+        }
       }
     }
 #pragma unroll
@@ -137,7 +150,7 @@ __global__ void k_bin_vertices(Dev D, BinCfg B) {
       if (pos != kEmpty) {
         D.bins[b][pos] = v;
         if (b == kNumBins - 1 && want_off)
-          D.hub_off[pos] = atomicAdd(&C->hub_cursor, next_pow2(2u * d));
+          D.hub_off[pos] = atomicAdd(&C->hub_cursor, cap);
       }
     }
     // pass accounting for the roofline: active vertices and their entries
@@ -168,7 +181,7 @@ __device__ __forceinline__ void emit_move(const Dev& D, bool move, uint32_t v, u
 }
 
 struct VtxCtx {
-  uint32_t rs, re, cv;
+  uint32_t rs, re, cv, ng;  // ng: vertices of v's graph at this level
   double kv, a_own, m, two_m2;
 };
 
@@ -180,8 +193,10 @@ __device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
   x.kv = D.k[v];
   x.a_own = D.a[x.cv];
   const uint32_t g = D.gid ? D.gid[v] : 0u;
-  x.m = D.gs[g].m;
-  x.two_m2 = D.gs[g].two_m2;
+  const GraphState& st = D.gs[g];
+  x.m = st.m;
+  x.two_m2 = st.two_m2;
+  x.ng = D.gid ? st.ve - st.vb : D.ctrl->n;
   return x;
 }
 
@@ -236,7 +251,7 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
       }
       best = team_max<T>(best, kFull);
     } else {
-      const uint32_t cap_v = live ? next_pow2(2u * (x.re - x.rs)) : 2u;
+      const uint32_t cap_v = live ? table_cap(x.re - x.rs, x.ng) : 2u;
       const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
       if (live)
         for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
@@ -329,7 +344,7 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
         }
       }
     } else {
-      const uint32_t cap_v = next_pow2(2u * (x.re - x.rs));
+      const uint32_t cap_v = table_cap(x.re - x.rs, x.ng);
       const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
       uint32_t* keys;
       Acc* vals;
@@ -375,7 +390,7 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
       if (c != x.cv && (!fast || v <= c)) {
         D.new_comm[v] = c;
         D.moved_it[v] = it;
-        D.movers[atomicAdd(&C->mover_count, 1u)] = v;
+        D.movers[C->n - 1u - atomicAdd(&C->hub_mover_count, 1u)] = v;
       }
     }
     __syncthreads();
@@ -392,13 +407,35 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
 // community.h:87-100 is kept incrementally: each directed entry (v,u) touching a mover
 // changes by w([post_v == post_u] - [pre_v == pre_u]); the mirror entry (u,v) is counted here
 // too when u did not move (factor 2).
+// Entries [e0, re) with stride `step` of mover v (old -> nw): activity push and the mover's
+// share of the internal-weight change.
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_apply(Dev D) {
+__device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t old, uint32_t nw,
+                                              uint32_t it, uint32_t e0, uint32_t re, uint32_t step,
+                                              long long& di, double& df) {
   using Tr = WTraits<WINT>;
   using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  for (uint32_t e = e0; e < re; e += step) {
+    const uint32_t u = D.col[e];
+    const uint32_t pre = D.comm[u];
+    const bool mu = D.moved_it[u] == it;
+    const uint32_t post = mu ? D.new_comm[u] : pre;
+    if (post != nw) D.active_it[u] = it + 1;
+    const int dd = (int)(nw == post) - (int)(old == pre);
+    if (dd) {
+      const int f = mu ? dd : 2 * dd;
+      if (WINT) di += (long long)f * (long long)w[e];
+      else df += (double)f * Tr::w_double(w[e]);
+    }
+  }
+}
+
+// One warp per mover found by the team kernels.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_apply(Dev D) {
   Ctrl* C = D.ctrl;
   const uint32_t count = C->mover_count, it = C->it;
-  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -413,20 +450,7 @@ __global__ void __launch_bounds__(256) k_apply(Dev D) {
     }
     long long di = 0;
     double df = 0.0;
-    const uint32_t rs = D.row[v], re = D.row[v + 1];
-    for (uint32_t e = rs + lane; e < re; e += 32) {
-      const uint32_t u = D.col[e];
-      const uint32_t pre = D.comm[u];
-      const bool mu = D.moved_it[u] == it;
-      const uint32_t post = mu ? D.new_comm[u] : pre;
-      if (post != nw) D.active_it[u] = it + 1;
-      const int dd = (int)(nw == post) - (int)(old == pre);
-      if (dd) {
-        const int f = mu ? dd : 2 * dd;
-        if (WINT) di += (long long)f * (long long)w[e];
-        else df += (double)f * Tr::w_double(w[e]);
-      }
-    }
+    apply_entries<WINT>(D, v, old, nw, it, D.row[v] + lane, D.row[v + 1], 32, di, df);
     if (WINT) {
       di = warp_sum(di);
       if (lane == 0 && di) atomicAdd(&D.gs[g].I, (unsigned long long)di);
@@ -437,15 +461,50 @@ __global__ void __launch_bounds__(256) k_apply(Dev D) {
   }
 }
 
+// One block per mover found by the block kernels (vertices with long rows).
+template <bool WINT>
+__global__ void __launch_bounds__(512) k_apply_hub(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->hub_mover_count, it = C->it, n = C->n;
+  __shared__ long long shi[32];
+  __shared__ double shf[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const uint32_t v = D.movers[n - 1u - idx];
+    const uint32_t old = D.comm[v], nw = D.new_comm[v];
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (threadIdx.x == 0) {
+      const double kv = D.k[v];
+      atomicAdd(&D.a[nw], kv);
+      atomicAdd(&D.a[old], -kv);
+    }
+    long long di = 0;
+    double df = 0.0;
+    apply_entries<WINT>(D, v, old, nw, it, D.row[v] + threadIdx.x, D.row[v + 1], blockDim.x, di, df);
+    di = warp_sum(di);
+    df = warp_sum(df);
+    if (lane == 0) { shi[wid] = di; shf[wid] = df; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long ti = 0;
+      double tf = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { ti += shi[i]; tf += shf[i]; }
+      if (WINT) { if (ti) atomicAdd(&D.gs[g].I, (unsigned long long)ti); }
+      else if (tf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[g].I), tf);
+    }
+    __syncthreads();
+  }
+}
+
 // ---- pass: commit moves and recompute sum_c a_c^2 -----------------------------------------------
 // Integer mode squares exactly in u64 (a_c <= 2m < 2^32). One graph: per-block partials,
 // summed in a fixed order by k_finalize. Several graphs: one block per graph.
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_commit_sq(Dev D, int single) {
   Ctrl* C = D.ctrl;
-  const uint32_t count = C->mover_count;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t v = D.movers[i];
+  const uint32_t count = C->mover_count, hubs = C->hub_mover_count, nn = C->n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count + hubs; i += gridDim.x * blockDim.x) {
+    const uint32_t v = D.movers[i < count ? i : nn - 1u - (i - count)];
     D.comm[v] = D.new_comm[v];
   }
   __shared__ double shd[33];
@@ -563,11 +622,11 @@ __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts
     st->iters += 1;
     st->total_iters += 1;
     if (single) {
-      st->moved = C->mover_count;
+      st->moved = C->mover_count + C->hub_mover_count;
       const uint32_t t = C->trace_len;
       if (t < kTraceCap) {
         TraceRec r;
-        r.level = st->level; r.iteration = st->iters - 1; r.n_moved = C->mover_count; r.pad = 0;
+        r.level = st->level; r.iteration = st->iters - 1; r.n_moved = st->moved; r.pad = 0;
         r.internal = I; r.sum_a2 = S; r.modularity = Q; r.delta = dq;
         C->trace[t] = r;
         C->trace_len = t + 1;
@@ -584,8 +643,9 @@ __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts
     C->loop_continue = tot > 0;
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->mover_count = 0;
+    C->hub_mover_count = 0;
     C->hub_cursor = 0;
-    for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
+    for (uint32_t i = 0; i < C->n_chunks && i < kMaxChunks; ++i) C->chunk_any[i] = 0;
     C->act_entries_total += C->act_entries;
     C->act_vertices_total += C->act_vertices;
     C->act_entries = 0;
@@ -617,6 +677,7 @@ __global__ void k_level_init(Dev D) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->mover_count = 0;
+    C->hub_mover_count = 0;
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
     for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
@@ -758,12 +819,15 @@ __global__ void k_fill_gid(uint32_t* gid, const long long* offs, uint32_t G) {
 
 // Hash-table arena needed by the global-table bin at this level: sum over vertices with
 // degree above the shared-memory bound of next_pow2(2 d).
-__global__ void k_arena_need(Dev D, uint32_t min_deg, unsigned long long* need) {
+__global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap, unsigned long long* need) {
   const uint32_t n = D.ctrl->n;
   unsigned long long s = 0;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const uint32_t d = D.row[v + 1] - D.row[v];
-    if (d > min_deg) s += next_pow2(2u * d);
+    if (d <= min_deg) continue;
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    const uint32_t cap = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
+    if (cap > block_cap) s += cap;
   }
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(need, s);
@@ -800,6 +864,7 @@ __global__ void k_agg_meta(Dev D) {
     const unsigned long long end = D.map[st->ve - 1];
     st->map_base = (uint32_t)(before >> 32);
     st->n_best = (uint32_t)(end >> 32) - st->map_base;
+    st->n_next = (uint32_t)end - (uint32_t)before;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) C->n_next = n ? (uint32_t)D.map[n - 1] : 0u;
 }
@@ -850,26 +915,154 @@ __global__ void k_agg_scatter(Dev D) {
   }
 }
 
-// Bin the new communities by their summed member degree (the contraction's work).
+// Capacity of a new community's contraction table: distinct destinations are bounded by the
+// member degree sum and by the graph's next-level vertex count. Global (bin 7) tables are
+// whole multiples of kHubChunk so every chunk of the arena belongs to one table.
+__device__ __forceinline__ uint32_t contract_cap(uint32_t dsum, uint32_t ng, bool global) {
+  const uint32_t c = table_cap(dsum, ng);
+  return global && c < kHubChunk ? kHubChunk : c;
+}
+
+// Bin the new communities by their summed member degree (the contraction's work). Bin 7
+// communities (the largest) are contracted by many blocks at once into a global table whose
+// arena offset is recorded per community in hubtab (kEmpty for every other community).
 __global__ void k_agg_bin(Dev D, BinCfg B) {
   Ctrl* C = D.ctrl;
   const uint32_t n2 = C->n_next;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n2; base += gridDim.x * blockDim.x) {
     const uint32_t s = base + threadIdx.x;
     int bin = -1;
-    uint32_t dsum = 0;
+    uint32_t dsum = 0, cap = 0;
     if (s < n2) {
       dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
       bin = bin_of(B, dsum);
+      if (bin == kNumBins - 1) {
+        const uint32_t g = D.gid ? D.gid[D.members[(uint32_t)(D.cd[s] >> 32)]] : 0u;
+        cap = contract_cap(dsum, D.gs[g].n_next, true);
+      }
     }
 #pragma unroll
     for (int b = 0; b < kNumBins; ++b) {
       const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
       if (pos != kEmpty) {
         D.bins[b][pos] = s;
-        if (b == kNumBins - 1) D.hub_off[pos] = atomicAdd(&C->hub_cursor, next_pow2(2u * dsum));
+        if (b == kNumBins - 1) {
+          const uint32_t off = atomicAdd(&C->hub_cursor, cap);
+          D.hub_off[pos] = off;
+          D.hubtab[s] = off;
+        }
       }
     }
+  }
+}
+
+// Bin-7 set-up once the arena is large enough: owner of every table chunk, and zeroed
+// accumulators (row length, k') of each such community.
+__global__ void k_hub_owner(Dev D, int bin) {
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[bin];
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const uint32_t s = D.bins[bin][idx];
+    const uint32_t v0 = D.members[(uint32_t)(D.cd[s] >> 32)];
+    const uint32_t g = D.gid ? D.gid[v0] : 0u;
+    const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
+    const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
+    const uint32_t c0 = D.hub_off[idx] / kHubChunk;
+    for (uint32_t j = threadIdx.x; j < cap / kHubChunk; j += blockDim.x) D.hub_owner[c0 + j] = s;
+    if (threadIdx.x == 0) {
+      D.newdeg[s] = 0;
+      D.kB[s] = 0.0;
+      if (D.gidB) D.gidB[s] = g;
+    }
+  }
+}
+
+// Bin-7 insert: one warp per member vertex, all members of all large communities at once,
+// into their communities' global tables (L2 atomics).
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_hub_insert(Dev D) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  Ctrl* C = D.ctrl;
+  const uint32_t n = C->n;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  Acc* vals = reinterpret_cast<Acc*>(D.arena_vals);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t err = 0;
+  for (uint32_t v = warp; v < n; v += nwarps) {
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    if (!D.gs[g].cont) continue;
+    const uint32_t s = D.new_comm[v];
+    const uint32_t off = D.hubtab[s];
+    if (off == kEmpty) continue;
+    const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
+    const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
+    if ((unsigned long long)off + cap > C->arena_slots) { err |= kErrArena; continue; }
+    const uint32_t mask = cap - 1u, shift = 32u - log2_pow2(cap);
+    const uint32_t re = D.row[v + 1];
+    for (uint32_t e = D.row[v] + lane; e < re; e += 32)
+      if (!table_add(D.arena_keys + off, vals + off, mask, shift, D.new_comm[D.col[e]], (Acc)w[e]))
+        err |= kErrTableFull;
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+// Bin-7 emit: one block per table chunk; occupied slots are appended to the community's row
+// (positions claimed with one atomic per block), k' and the self-loop weight accumulated.
+template <bool WINT>
+__global__ void __launch_bounds__(512) k_hub_emit(Dev D, uint32_t nchunks) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  __shared__ uint32_t shu[33];
+  __shared__ double shd[33];
+  __shared__ uint32_t base_sh;
+  Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
+  const Acc* vals = reinterpret_cast<const Acc*>(D.arena_vals);
+  constexpr int PER = kHubChunk / 512;
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const uint32_t s = D.hub_owner[c];
+    const uint32_t tb = (uint32_t)D.cd[s];
+    const uint32_t v0 = D.members[(uint32_t)(D.cd[s] >> 32)];
+    const uint32_t g = D.gid ? D.gid[v0] : 0u;
+    const uint32_t slot0 = c * kHubChunk + threadIdx.x * PER;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) cnt += D.arena_keys[slot0 + i] != kEmpty;
+    uint32_t total;
+    uint32_t off = block_excl_scan<uint32_t, 512>(cnt, shu, &total);
+    if (threadIdx.x == 0) base_sh = total ? atomicAdd(&D.newdeg[s], total) : 0u;
+    __syncthreads();
+    off += base_sh;
+    double ksum = 0.0, self = 0.0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const uint32_t d = D.arena_keys[slot0 + i];
+      if (d == kEmpty) continue;
+      const Acc sum = vals[slot0 + i];
+      Wt wv;
+      if (WINT) wv = (Wt)sum;
+      else wv = (Wt)__double2float_rn((double)sum);
+      D.colB[tb + off] = d;
+      wout[tb + off] = wv;
+      ++off;
+      ksum += Tr::w_double(wv);
+      if (d == s) self += Tr::w_double(wv);
+    }
+    double ktot, stot;
+    block_excl_scan<double, 512>(ksum, shd, &ktot);
+    block_excl_scan<double, 512>(self, shd, &stot);
+    if (threadIdx.x == 0) {
+      if (ktot != 0.0) atomicAdd(&D.kB[s], ktot);
+      if (stot != 0.0) {
+        if (WINT) atomicAdd(&D.gs[g].I, (unsigned long long)stot);
+        else atomicAdd(reinterpret_cast<double*>(&D.gs[g].I), stot);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -916,7 +1109,7 @@ __global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t 
     const uint32_t s = live ? list[idx] : 0u;
     CommCtx x{};
     if (live) x = load_comm(D, s);
-    const uint32_t cap_v = live ? next_pow2(2u * (x.dsum > 0 ? x.dsum : 1u)) : 2u;
+    const uint32_t cap_v = live ? contract_cap(x.dsum, D.gs[x.g].n_next, false) : 2u;
     const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
     if (live)
       for (uint32_t i = lane; i < cap_v; i += T) { keys[i] = kEmpty; vals[i] = Acc(0); }
@@ -975,7 +1168,8 @@ __global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t 
   if (err) atomicOr(&C->err, err);
 }
 
-template <bool WINT, bool GTABLE>
+// One block per new community of bin 6 (shared-memory table).
+template <bool WINT>
 __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t cap) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
@@ -993,17 +1187,12 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
     const uint32_t s = list[idx];
     const CommCtx x = load_comm(D, s);
-    const uint32_t cap_v = next_pow2(2u * (x.dsum > 0 ? x.dsum : 1u));
+    const uint32_t cap_v = contract_cap(x.dsum, D.gs[x.g].n_next, false);
     const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
     uint32_t* keys;
     Acc* vals;
     bool ok;
-    if (GTABLE) {
-      const uint32_t off = D.hub_off[idx];
-      ok = (unsigned long long)off + cap_v <= C->arena_slots;
-      keys = D.arena_keys + off;
-      vals = reinterpret_cast<Acc*>(D.arena_vals) + off;
-    } else {
+    {
       ok = cap_v <= cap;
       keys = reinterpret_cast<uint32_t*>(smem);
       vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
