@@ -198,6 +198,23 @@ typedef struct {
 /* Copies up to `cap` records (oldest first) and sets *len to the number recorded. */
 lv_status lv_community_get_trace(lv_community* c, lv_trace_record* out, int32_t cap, int32_t* len);
 
+/* ---- allocation-free modularity ----------------------------------------------------------
+ * No counterpart in the reference. For callers that may not allocate device memory when they
+ * call (a framework that owns all of HBM through its own pool, a serving loop that must not
+ * stall on cudaMalloc): Q = I/(2m) - S/(4 m m) of partition `comm` (int32[n], labels in
+ * [0, n)) on the CSR graph, with every buffer in device memory. Uses only the caller's buffers
+ * and one scratch array compiled into the library (LV_NOALLOC_MAX_VERTICES + 64 words of 8
+ * bytes, held on each GPU that loads the library until the process exits); n above
+ * LV_NOALLOC_MAX_VERTICES returns LV_ERR_RANGE before anything runs. Writes out[0..3] =
+ * {Q, I, S, m} (device memory; Q is NaN if a label is out of range) asynchronously on
+ * `stream` (a cudaStream_t, NULL = default stream). The first call on a device looks up the
+ * scratch array's address; make it before any stream capture. Calls that overlap on the GPU
+ * share the scratch array and race. weights_integer != 0 (or w == NULL) sums exactly in u64
+ * like LV_WEIGHTS_INTEGER; otherwise in double. */
+#define LV_NOALLOC_MAX_VERTICES 1048576
+lv_status lv_modularity_noalloc(int64_t n, const int64_t* row_ptr, const int32_t* col, const float* w,
+                                const int32_t* comm, int32_t weights_integer, double* out, void* stream);
+
 /* ---- serving ---------------------------------------------------------------------------
  * Continuous batching with graph state resident in HBM. No reference counterpart.
  * Requests are admitted while the device memory they need fits `budget_bytes` and a slot is
