@@ -3,10 +3,25 @@
 // reductions and scans.
 #pragma once
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace lv {
+
+namespace cg = cooperative_groups;
+
+// Warp aggregation of a keyed update: the active lanes holding the same key add their values
+// together and one of them passes (key, sum) to `sink`. Turns up to 32 atomics on one hot
+// address into one. Callable from divergent code.
+template <class K, class V, class F>
+__device__ __forceinline__ void warp_combine(K key, V val, F&& sink) {
+  const cg::coalesced_group act = cg::coalesced_threads();
+  const auto grp = cg::labeled_partition(act, key);
+  const V sum = cg::reduce(grp, val, cg::plus<V>());
+  if (grp.thread_rank() == 0) sink(key, sum);
+}
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;  // empty hash slot / no community
 constexpr uint32_t kNever = 0xFFFFFFFFu;  // iteration stamp that never matches
@@ -79,6 +94,7 @@ struct Ctrl {
   uint32_t bin_count[kNumBins];
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
+  uint32_t long_count;         // aggregation: pieces of long rows for k_hub_insert_long
   uint32_t hub_cursor;         // global hash-table arena cursor (slots)
   uint32_t arena_slots;        // arena capacity (slots)
   uint32_t n_next, E_next;     // aggregation outputs
@@ -202,6 +218,45 @@ __device__ __forceinline__ unsigned long long team_max(unsigned long long x, uns
     const unsigned long long y = __shfl_xor_sync(mask, x, o);
     x = y > x ? y : x;
   }
+  return x;
+}
+
+// Load-balanced walk over the rows of up to 32 vertices held one per lane: calls
+// f(entry index, pa, pb) for every entry of every row -- pa/pb being the payload of the lane
+// that owns the row -- with all 32 lanes busy however the row lengths are spread. Lane i holds
+// (rs_i, len_i, pa_i, pb_i); every lane of the warp must call it.
+template <class F>
+__device__ __forceinline__ void warp_expand_rows(uint32_t rs, uint32_t len, uint32_t pa, uint32_t pb,
+                                                 F&& f) {
+  const int lane = threadIdx.x & 31;
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t excl = incl - len;
+  for (uint32_t jb = 0; jb < total; jb += 32) {
+    const uint32_t j = jb + lane;
+    // owner lane: the last lane whose exclusive offset is <= j
+    int k = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const uint32_t ex = __shfl_sync(kFull, excl, k + step);
+      if (ex <= j) k += step;
+    }
+    const uint32_t base = __shfl_sync(kFull, rs, k) - __shfl_sync(kFull, excl, k);
+    const uint32_t a = __shfl_sync(kFull, pa, k), b = __shfl_sync(kFull, pb, k);
+    if (j < total) f(base + j, a, b);
+  }
+}
+
+// Sum over the aligned group of T lanes (every lane of the warp must call it).
+template <int T, class V>
+__device__ __forceinline__ V team_sum(V x) {
+#pragma unroll
+  for (int o = T / 2; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
   return x;
 }
 

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -147,6 +148,7 @@ class Run {
   int32_t levels_run = 0;
   double t_opt_ms = 0, t_agg_ms = 0, t_opt0 = -1, t_agg0 = -1, t_optk_ms = 0;
   int64_t launches = 0;
+  bool debug = std::getenv("LV_DEBUG") != nullptr;  // per-level sizes and bin populations on stderr
   cudaEvent_t ev[6];
   std::vector<Block> arena_blocks;
 
@@ -283,6 +285,8 @@ class Run {
     for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned,n);
     D.hub_off = dalloc<uint32_t>(ctx, owned,n);
     D.hubtab = dalloc<uint32_t>(ctx, owned, n);
+    D.hubself = dalloc<unsigned long long>(ctx, owned, n);
+    D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
     D.movers = dalloc<uint32_t>(ctx, owned,n);
     D.gs = dalloc<GraphState>(ctx, owned,G);
     D.ctrl = dalloc<Ctrl>(ctx, owned,1);
@@ -366,9 +370,11 @@ class Run {
     iota_best();
     if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
     else k_prep<false><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
+    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(D, w_dev_tmp);
+    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(D, w_dev_tmp);
     if (wint) k_prep_total<true><<<1, 256, 0, st>>>(D);
     else k_prep_total<false><<<1, 256, 0, st>>>(D);
-    launches += 3 + (G > 1 ? 1 : 0) + (w && cfg.weight_mode == LV_WEIGHTS_AUTO ? 1 : 0);
+    launches += 4 + (G > 1 ? 1 : 0) + (w && cfg.weight_mode == LV_WEIGHTS_AUTO ? 1 : 0);
     check_device_errors();
     level_start();
   }
@@ -502,6 +508,13 @@ class Run {
       LV_CUDA(cudaMemsetAsync(D.hubtab, 0xFF, (size_t)n2 * 4, st));
       k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
       const uint32_t need = ctrl_u32(offsetof(Ctrl, hub_cursor));
+      if (debug) {
+        uint32_t bc[kNumBins];
+        LV_CUDA(cudaMemcpy(bc, reinterpret_cast<char*>(D.ctrl) + offsetof(Ctrl, bin_count), sizeof(bc), cudaMemcpyDeviceToHost));
+        std::fprintf(stderr, "[lv] contract n=%u E=%u -> n'=%u bins", n, E, n2);
+        for (uint32_t b : bc) std::fprintf(stderr, " %u", b);
+        std::fprintf(stderr, " hub_slots=%u\n", need);
+      }
       ensure_arena(need);
       if (need > 0) {
         // the largest new communities: many blocks insert into their global tables
@@ -509,8 +522,9 @@ class Run {
         LV_CUDA(cudaMemsetAsync(D.arena_vals, 0, (size_t)need * 8, st));
         k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(D, kNumBins - 1);
         k_hub_insert<WI><<<grid_n, 256, 0, st>>>(D);
+        k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
         k_hub_emit<WI><<<std::min<uint32_t>(need / kHubChunk, (uint32_t)ctx->sms * 8), 512, 0, st>>>(D, need / kHubChunk);
-        launches += 3;
+        launches += 4;
       }
       k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
       k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);

@@ -32,6 +32,8 @@ struct Dev {
   uint32_t* bins[kNumBins];
   uint32_t* hub_off;    // [n] arena offset per entry of the global-table bin
   uint32_t* hubtab;     // [n] aggregation: arena offset of each bin-7 new community, else kEmpty
+  unsigned long long* hubself;  // [n] aggregation: self-loop weight of each bin-7 community
+  unsigned long long* long_items;  // [n + E/kHubPiece + 16] (vertex << 32 | piece) of long rows
   uint32_t* movers;     // [n]
   uint32_t* arena_keys;
   void* arena_vals;     // 8 bytes per slot
@@ -62,6 +64,9 @@ struct BinCfg {
 
 // Table granule of the multi-block global tables: every global table is a multiple of it.
 constexpr uint32_t kHubChunk = 4096;
+// Rows longer than kHubLongRow entries are inserted in pieces of kHubPiece by separate blocks.
+constexpr uint32_t kHubLongRow = 2048;
+constexpr uint32_t kHubPiece = 8192;
 
 constexpr int kMaxPartials = 2048;
 
@@ -256,16 +261,21 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
       if (live)
         for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
       __syncwarp();
+      // weight into the vertex's own community stays in registers (it is the hottest key)
+      Acc self_acc = Acc(0);
       if (live) {
         for (uint32_t e = x.rs + lane; e < x.re; e += T) {
           const uint32_t u = D.col[e];
           if (u == v) continue;
-          if (!table_add(keys, vals, mask, shift, D.comm[u], (Acc)w[e])) err |= kErrTableFull;
+          const uint32_t cu = D.comm[u];
+          if (cu == x.cv) { self_acc += (Acc)w[e]; continue; }
+          if (!table_add(keys, vals, mask, shift, cu, (Acc)w[e])) err |= kErrTableFull;
         }
       }
+      self_acc = team_sum<T>(self_acc);
       __syncwarp();
       if (live) {
-        const float self_v = Tr::to_float(table_get(keys, vals, mask, shift, x.cv));
+        const float self_v = Tr::to_float(self_acc);
         for (uint32_t s = lane; s < cap_v; s += T) {
           const uint32_t c = keys[s];
           if (c == kEmpty || c == x.cv) continue;
@@ -288,6 +298,25 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
     emit_move(D, move, v, c, it);
   }
   if (err) atomicOr(&C->err, err);
+}
+
+// Block-wide sum (all threads call; result valid in every thread; `sh` holds >= 33 values).
+// The reduction tree is fixed, so a double sum is the same on every run.
+template <int NT, class V>
+__device__ __forceinline__ V block_sum(V x, V* sh) {
+  x = warp_sum(x);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    V y = lane < NT / 32 ? sh[lane] : V(0);
+    y = warp_sum(y);
+    if (lane == 0) sh[32] = y;
+  }
+  __syncthreads();
+  const V r = sh[32];
+  __syncthreads();
+  return r;
 }
 
 // Block-wide max of a u64 (all threads call; result valid in every thread).
@@ -363,16 +392,19 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
       if (ok)
         for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
       __syncthreads();
+      Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
       if (ok) {
         for (uint32_t e = x.rs + threadIdx.x; e < x.re; e += NT) {
           const uint32_t u = D.col[e];
           if (u == v) continue;
-          if (!table_add(keys, vals, mask, shift, D.comm[u], (Acc)w[e])) err |= kErrTableFull;
+          const uint32_t cu = D.comm[u];
+          if (cu == x.cv) { self_acc += (Acc)w[e]; continue; }
+          if (!table_add(keys, vals, mask, shift, cu, (Acc)w[e])) err |= kErrTableFull;
         }
       }
-      __syncthreads();
+      self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
       if (ok) {
-        const float self_v = Tr::to_float(table_get(keys, vals, mask, shift, x.cv));
+        const float self_v = Tr::to_float(self_acc);
         for (uint32_t s = threadIdx.x; s < cap_v; s += NT) {
           const uint32_t c = keys[s];
           if (c == kEmpty || c == x.cv) continue;
@@ -720,6 +752,34 @@ __global__ void k_chunk_bounds(Dev D, unsigned long long step) {
 // ---- level 0: input validation, weights, k, self-loop weight, total weight --------------------------
 // GraphDevice(GraphHost&) (graph.cuh:46-99) and the Community constructor (community.h:31-46):
 // k = sum of incident weights, m = total weight / 2 (graph.cu:81). One warp per vertex.
+constexpr uint32_t kPrepLongRow = 4096;
+
+// Validation and weight conversion of entries [e0, re) with stride `step` of row v (graph
+// vertex range [lo, hi)); sums of the row's weights and of its self-loop weights.
+template <bool WINT>
+__device__ __forceinline__ void prep_entries(const Dev& D, uint32_t v, long long e0, long long re,
+                                             uint32_t step, uint32_t lo, uint32_t hi, const float* wf_in,
+                                             unsigned long long& ki, unsigned long long& si,
+                                             double& kf, double& sf, uint32_t& err) {
+  for (long long e = e0; e < re; e += step) {
+    const uint32_t u = D.col[e];
+    if (u < lo || u >= hi) { err |= kErrInput; continue; }
+    const float x = wf_in ? wf_in[e] : 1.0f;
+    if (WINT) {
+      if (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f) { err |= kErrInput; continue; }
+      const uint32_t xi = (uint32_t)x;
+      reinterpret_cast<uint32_t*>(D.w)[e] = xi;
+      ki += xi;
+      if (u == v) si += xi;
+    } else {
+      if (!(x > 0.0f) || !(x < INFINITY)) { err |= kErrInput; continue; }
+      reinterpret_cast<float*>(D.w)[e] = x;
+      kf += (double)x;
+      if (u == v) sf += (double)x;
+    }
+  }
+}
+
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, const float* wf_in,
                                               uint32_t n, unsigned long long E) {
@@ -728,6 +788,20 @@ __global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, con
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t err = 0;
+  // per-graph totals are kept in registers and flushed when the graph changes
+  uint32_t cur_g = kEmpty;
+  unsigned long long tk_i = 0, ts_i = 0;
+  double tk_f = 0.0, ts_f = 0.0;
+  auto flush = [&]() {
+    if (cur_g == kEmpty || lane != 0) return;
+    if (WINT) {
+      if (ts_i) atomicAdd(&D.gs[cur_g].I, ts_i);
+      if (tk_i) atomicAdd(&D.gs[cur_g].S, tk_i);  // S holds sum k (= 2m) until k_prep_total
+    } else {
+      if (ts_f != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[cur_g].I), ts_f);
+      if (tk_f != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[cur_g].S), tk_f);
+    }
+  };
   for (uint32_t v = warp; v < n; v += nwarps) {
     const long long rs = row64[v], re = row64[v + 1];
     const uint32_t g = D.gid ? D.gid[v] : 0u;
@@ -740,37 +814,64 @@ __global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, con
       D.row[v] = (uint32_t)rs;
       if (v == n - 1) D.row[n] = (uint32_t)re;
     }
+    if (re - rs > kPrepLongRow) {  // a block takes it (k_prep_long)
+      if (lane == 0) D.bins[kNumBins - 1][atomicAdd(&C->bin_count[kNumBins - 1], 1u)] = v;
+      continue;
+    }
+    if (g != cur_g) {
+      flush();
+      cur_g = g;
+      tk_i = ts_i = 0;
+      tk_f = ts_f = 0.0;
+    }
     unsigned long long ki = 0, si = 0;
     double kf = 0.0, sf = 0.0;
-    for (long long e = rs + lane; e < re; e += 32) {
-      const uint32_t u = D.col[e];
-      if (u < lo || u >= hi) { err |= kErrInput; continue; }
-      const float x = wf_in ? wf_in[e] : 1.0f;
-      if (WINT) {
-        if (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f) { err |= kErrInput; continue; }
-        const uint32_t xi = (uint32_t)x;
-        reinterpret_cast<uint32_t*>(D.w)[e] = xi;
-        ki += xi;
-        if (u == v) si += xi;
-      } else {
-        if (!(x > 0.0f) || !(x < INFINITY)) { err |= kErrInput; continue; }
-        reinterpret_cast<float*>(D.w)[e] = x;
-        kf += (double)x;
-        if (u == v) sf += (double)x;
-      }
-    }
+    prep_entries<WINT>(D, v, rs + lane, re, 32, lo, hi, wf_in, ki, si, kf, sf, err);
     if (WINT) {
       ki = warp_sum(ki);
       si = warp_sum(si);
-      if (lane == 0) {
-        D.k[v] = (double)ki;
-        if (si) atomicAdd(&D.gs[g].I, si);
-        atomicAdd(&D.gs[g].S, ki);  // S temporarily holds sum k (= 2m) until k_prep_total
-      }
+      if (lane == 0) D.k[v] = (double)ki;
+      tk_i += ki;
+      ts_i += si;
     } else {
       kf = warp_sum(kf);
       sf = warp_sum(sf);
-      if (lane == 0) {
+      if (lane == 0) D.k[v] = kf;
+      tk_f += kf;
+      ts_f += sf;
+    }
+  }
+  flush();
+  if (err) atomicOr(&C->err, err);
+}
+
+// Rows longer than kPrepLongRow entries, one block each.
+template <bool WINT>
+__global__ void __launch_bounds__(512) k_prep_long(Dev D, const float* wf_in) {
+  Ctrl* C = D.ctrl;
+  __shared__ unsigned long long shu[33];
+  __shared__ double shd[33];
+  const uint32_t count = C->bin_count[kNumBins - 1];
+  uint32_t err = 0;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const uint32_t v = D.bins[kNumBins - 1][idx];
+    const uint32_t rs = D.row[v], re = D.row[v + 1];
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    unsigned long long ki = 0, si = 0;
+    double kf = 0.0, sf = 0.0;
+    prep_entries<WINT>(D, v, rs + threadIdx.x, re, blockDim.x, D.gs[g].vb, D.gs[g].ve, wf_in, ki, si, kf, sf, err);
+    if (WINT) {
+      ki = block_sum<512>(ki, shu);
+      si = block_sum<512>(si, shu);
+      if (threadIdx.x == 0) {
+        D.k[v] = (double)ki;
+        if (si) atomicAdd(&D.gs[g].I, si);
+        atomicAdd(&D.gs[g].S, ki);
+      }
+    } else {
+      kf = block_sum<512>(kf, shd);
+      sf = block_sum<512>(sf, shd);
+      if (threadIdx.x == 0) {
         D.k[v] = kf;
         if (sf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gs[g].I), sf);
         atomicAdd(reinterpret_cast<double*>(&D.gs[g].S), kf);
@@ -969,9 +1070,11 @@ __global__ void k_hub_owner(Dev D, int bin) {
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     const uint32_t c0 = D.hub_off[idx] / kHubChunk;
     for (uint32_t j = threadIdx.x; j < cap / kHubChunk; j += blockDim.x) D.hub_owner[c0 + j] = s;
+    if (blockIdx.x == 0 && idx == 0 && threadIdx.x == 0) C->long_count = 0;
     if (threadIdx.x == 0) {
       D.newdeg[s] = 0;
       D.kB[s] = 0.0;
+      D.hubself[s] = 0ull;
       if (D.gidB) D.gidB[s] = g;
     }
   }
@@ -992,20 +1095,98 @@ __global__ void __launch_bounds__(256) k_hub_insert(Dev D) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t err = 0;
-  for (uint32_t v = warp; v < n; v += nwarps) {
-    const uint32_t g = D.gid ? D.gid[v] : 0u;
-    if (!D.gs[g].cont) continue;
-    const uint32_t s = D.new_comm[v];
-    const uint32_t off = D.hubtab[s];
-    if (off == kEmpty) continue;
+  // a warp takes 32 consecutive vertices; the rows of those in large communities are spread
+  // over its lanes. Entries staying inside their community are summed in registers.
+  uint32_t self_s = kEmpty;  // per-lane running self-loop sum, flushed when the community changes
+  Acc self_acc = Acc(0);
+  auto flush_self = [&]() {
+    if (self_s == kEmpty || self_acc == Acc(0)) return;
+    if (WINT) atomicAdd(&D.hubself[self_s], (unsigned long long)self_acc);
+    else atomicAdd(reinterpret_cast<double*>(&D.hubself[self_s]), (double)self_acc);
+  };
+  auto add = [&](uint32_t e, uint32_t s, uint32_t off) {
+    const uint32_t d = D.new_comm[D.col[e]];
+    if (d == s) {
+      if (s != self_s) {
+        flush_self();
+        self_s = s;
+        self_acc = Acc(0);
+      }
+      self_acc += (Acc)w[e];
+      return;
+    }
+    const uint32_t g = D.gid ? D.gid[D.col[e]] : 0u;
     const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
-    if ((unsigned long long)off + cap > C->arena_slots) { err |= kErrArena; continue; }
+    if (!table_add(D.arena_keys + off, vals + off, cap - 1u, 32u - log2_pow2(cap), d, (Acc)w[e]))
+      err |= kErrTableFull;
+  };
+  for (uint32_t vb = warp * 32u; vb < n; vb += nwarps * 32u) {
+    const uint32_t v = vb + lane;
+    uint32_t rs = 0, len = 0, s = 0, off = kEmpty;
+    if (v < n) {
+      const uint32_t g = D.gid ? D.gid[v] : 0u;
+      if (D.gs[g].cont) {
+        s = D.new_comm[v];
+        off = D.hubtab[s];
+        if (off != kEmpty) {
+          const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
+          const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
+          if ((unsigned long long)off + cap > C->arena_slots) err |= kErrArena;
+          else {
+            rs = D.row[v];
+            len = D.row[v + 1] - rs;
+            if (len > kHubLongRow) {
+              // long rows are cut into pieces that separate blocks insert (k_hub_insert_long)
+              const uint32_t np = (len + kHubPiece - 1) / kHubPiece;
+              const uint32_t p0 = atomicAdd(&C->long_count, np);
+              for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
+              len = 0;
+            }
+          }
+        }
+      }
+    }
+    warp_expand_rows(rs, len, s, off, add);
+  }
+  flush_self();
+  if (err) atomicOr(&C->err, err);
+}
+
+// Pieces of the long rows deferred by k_hub_insert, one block per piece.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_hub_insert_long(Dev D) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  __shared__ Acc sh[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->long_count;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  Acc* vals = reinterpret_cast<Acc*>(D.arena_vals);
+  uint32_t err = 0;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const unsigned long long it = D.long_items[idx];
+    const uint32_t v = (uint32_t)(it >> 32), piece = (uint32_t)it;
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    const uint32_t s = D.new_comm[v];
+    const uint32_t off = D.hubtab[s];
+    const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
+    const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     const uint32_t mask = cap - 1u, shift = 32u - log2_pow2(cap);
-    const uint32_t re = D.row[v + 1];
-    for (uint32_t e = D.row[v] + lane; e < re; e += 32)
-      if (!table_add(D.arena_keys + off, vals + off, mask, shift, D.new_comm[D.col[e]], (Acc)w[e]))
-        err |= kErrTableFull;
+    const uint32_t rs = D.row[v] + piece * kHubPiece;
+    const uint32_t re = min(D.row[v + 1], rs + kHubPiece);
+    Acc self_acc = Acc(0);
+    for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
+      const uint32_t d = D.new_comm[D.col[e]];
+      if (d == s) { self_acc += (Acc)w[e]; continue; }
+      if (!table_add(D.arena_keys + off, vals + off, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+    }
+    self_acc = block_sum<256>(self_acc, sh);
+    if (threadIdx.x == 0 && self_acc != Acc(0)) {
+      if (WINT) atomicAdd(&D.hubself[s], (unsigned long long)self_acc);
+      else atomicAdd(reinterpret_cast<double*>(&D.hubself[s]), (double)self_acc);
+    }
   }
   if (err) atomicOr(&C->err, err);
 }
@@ -1056,6 +1237,18 @@ __global__ void __launch_bounds__(512) k_hub_emit(Dev D, uint32_t nchunks) {
     block_excl_scan<double, 512>(ksum, shd, &ktot);
     block_excl_scan<double, 512>(self, shd, &stot);
     if (threadIdx.x == 0) {
+      // the community's first chunk also emits its self-loop, summed outside the table
+      if (c == D.hubtab[s] / kHubChunk && D.hubself[s] != 0ull) {
+        const unsigned long long hs = D.hubself[s];
+        Wt wv;
+        if (WINT) wv = (Wt)hs;
+        else wv = (Wt)__double2float_rn(__longlong_as_double((long long)hs));
+        const uint32_t pos = atomicAdd(&D.newdeg[s], 1u);
+        D.colB[tb + pos] = s;
+        wout[tb + pos] = wv;
+        ktot += Tr::w_double(wv);
+        stot += Tr::w_double(wv);
+      }
       if (ktot != 0.0) atomicAdd(&D.kB[s], ktot);
       if (stot != 0.0) {
         if (WINT) atomicAdd(&D.gs[g].I, (unsigned long long)stot);
@@ -1114,16 +1307,35 @@ __global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t 
     if (live)
       for (uint32_t i = lane; i < cap_v; i += T) { keys[i] = kEmpty; vals[i] = Acc(0); }
     __syncwarp();
-    if (live) {
+    // entries staying inside the community (the new self-loop, the hottest key) are summed in
+    // registers; only entries to other communities go through the table
+    Acc self_acc = Acc(0);
+    auto add = [&](uint32_t e, uint32_t, uint32_t) {
+      const uint32_t d = D.new_comm[D.col[e]];
+      if (d == s) { self_acc += (Acc)w[e]; return; }
+      if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+    };
+    if (T == 32) {
+      // a warp per community: members taken 32 at a time, their entries spread over all lanes
+      if (live) {
+        for (uint32_t gb = x.mb; gb < x.me; gb += 32) {
+          uint32_t rs = 0, len = 0;
+          if (gb + lane < x.me) {
+            const uint32_t v = D.members[gb + lane];
+            rs = D.row[v];
+            len = D.row[v + 1] - rs;
+          }
+          warp_expand_rows(rs, len, 0u, 0u, add);
+        }
+      }
+    } else if (live) {
       for (uint32_t i = x.mb; i < x.me; ++i) {
         const uint32_t v = D.members[i];
         const uint32_t re = D.row[v + 1];
-        for (uint32_t e = D.row[v] + lane; e < re; e += T) {
-          const uint32_t d = D.new_comm[D.col[e]];
-          if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
-        }
+        for (uint32_t e = D.row[v] + lane; e < re; e += T) add(e, 0u, 0u);
       }
     }
+    self_acc = team_sum<T>(self_acc);
     __syncwarp();
     // compact the occupied slots of this team's table into the output row
     uint32_t cnt = 0;
@@ -1150,16 +1362,23 @@ __global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t 
         wout[x.tb + off] = wv;
         ++off;
         ksum += Tr::w_double(wv);
-        if (d == s) {
-          if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
-          else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), (double)wv);
-        }
       }
     }
 #pragma unroll
     for (int o = T / 2; o > 0; o >>= 1) ksum += __shfl_xor_sync(kFull, ksum, o, T);
     if (live && lane == 0) {
-      D.newdeg[s] = total;
+      const bool has_self = self_acc != Acc(0);  // weights are positive
+      if (has_self) {
+        Wt wv;
+        if (WINT) wv = (Wt)self_acc;
+        else wv = (Wt)__double2float_rn((double)self_acc);
+        D.colB[x.tb + total] = s;
+        wout[x.tb + total] = wv;
+        ksum += Tr::w_double(wv);
+        if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
+        else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), Tr::w_double(wv));
+      }
+      D.newdeg[s] = total + (has_self ? 1u : 0u);
       D.kB[s] = ksum;
       if (D.gidB) D.gidB[s] = x.g;
     }
@@ -1178,6 +1397,7 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t shu[33];
   __shared__ double shd[33];
+  __shared__ uint32_t mrs[NT], mex[NT];  // row start / entry offset of the members in flight
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
   const uint32_t* list = D.bins[bin];
@@ -1201,19 +1421,41 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
     if (ok)
       for (uint32_t i = threadIdx.x; i < cap_v; i += NT) { keys[i] = kEmpty; vals[i] = Acc(0); }
     __syncthreads();
+    Acc self_acc = Acc(0);  // entries staying inside the community, kept out of the table
     if (ok) {
-      // members with small rows: one member per warp lane group; long rows: whole block
-      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      for (uint32_t i = x.mb + wid; i < x.me; i += NT / 32) {
-        const uint32_t v = D.members[i];
-        const uint32_t re = D.row[v + 1];
-        for (uint32_t e = D.row[v] + lane; e < re; e += 32) {
-          const uint32_t d = D.new_comm[D.col[e]];
-          if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+      auto add = [&](uint32_t e, uint32_t, uint32_t) {
+        const uint32_t d = D.new_comm[D.col[e]];
+        if (d == s) { self_acc += (Acc)w[e]; return; }
+        if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+      };
+      // members taken NT at a time; their entries spread evenly over the whole block, each
+      // thread finding its entry's member by binary search in shared memory
+      for (uint32_t base = x.mb; base < x.me; base += NT) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t rs = 0, len = 0;
+        if (i < x.me) {
+          const uint32_t v = D.members[i];
+          rs = D.row[v];
+          len = D.row[v + 1] - rs;
         }
+        uint32_t total;
+        const uint32_t ex = block_excl_scan<uint32_t, NT>(len, shu, &total);
+        mrs[threadIdx.x] = rs;
+        mex[threadIdx.x] = ex;
+        __syncthreads();
+        const uint32_t cnt = min((uint32_t)NT, x.me - base);
+        for (uint32_t j = threadIdx.x; j < total; j += NT) {
+          uint32_t lo = 0, hi = cnt;
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (mex[mid] <= j) lo = mid; else hi = mid;
+          }
+          add(mrs[lo] + (j - mex[lo]), 0u, 0u);
+        }
+        __syncthreads();
       }
     }
-    __syncthreads();
+    self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(shd));
     uint32_t cnt = 0;
     if (ok)
       for (uint32_t i = threadIdx.x; i < cap_v; i += NT) cnt += keys[i] != kEmpty;
@@ -1232,16 +1474,23 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
         wout[x.tb + off] = wv;
         ++off;
         ksum += Tr::w_double(wv);
-        if (d == s) {
-          if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
-          else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), (double)wv);
-        }
       }
     }
     double ktot;
     block_excl_scan<double, NT>(ksum, shd, &ktot);
     if (threadIdx.x == 0) {
-      D.newdeg[s] = ok ? total : 0u;
+      const bool has_self = ok && self_acc != Acc(0);  // weights are positive
+      if (has_self) {
+        Wt wv;
+        if (WINT) wv = (Wt)self_acc;
+        else wv = (Wt)__double2float_rn((double)self_acc);
+        D.colB[x.tb + total] = s;
+        wout[x.tb + total] = wv;
+        ktot += Tr::w_double(wv);
+        if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
+        else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), Tr::w_double(wv));
+      }
+      D.newdeg[s] = ok ? total + (has_self ? 1u : 0u) : 0u;
       D.kB[s] = ktot;
       if (D.gidB) D.gidB[s] = x.g;
     }
@@ -1251,26 +1500,52 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
 }
 
 // Copy the gapped contracted rows into the dense next-level CSR (col/w), move k' and gid'.
+// The output is cut into chunks of kCompactChunk entries, one block per chunk, so a row of any
+// length is copied by as many blocks as it spans; each block stages the row offsets that
+// overlap its chunk in shared memory and finds every entry's row by binary search there.
+constexpr uint32_t kCompactChunk = 2048;
+
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_agg_compact(Dev D) {
   using Wt = typename WTraits<WINT>::W;
+  __shared__ uint32_t rs[kCompactChunk + 2];
+  __shared__ uint32_t r0_sh, nr_sh;
   Ctrl* C = D.ctrl;
   const uint32_t n2 = C->n_next;
-  const int lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t E2 = D.rowB[n2];
   const Wt* __restrict__ win = reinterpret_cast<const Wt*>(D.wB);
   Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.w);
-  for (uint32_t s = warp; s < n2; s += nwarps) {
-    const uint32_t src = (uint32_t)D.cd[s], dst = D.rowB[s], len = D.rowB[s + 1] - dst;
-    for (uint32_t i = lane; i < len; i += 32) {
-      D.col[dst + i] = D.colB[src + i];
-      wout[dst + i] = win[src + i];
+  const uint32_t nchunks = (E2 + kCompactChunk - 1) / kCompactChunk;
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const uint32_t start = ch * kCompactChunk;
+    const uint32_t end = min(start + kCompactChunk, E2);
+    if (threadIdx.x == 0) {
+      uint32_t lo = 0, hi = n2;  // last row with rowB[r] <= start
+      while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (D.rowB[mid] <= start) lo = mid; else hi = mid; }
+      uint32_t r1 = lo;           // first row with rowB[r] >= end
+      hi = n2;
+      uint32_t lo2 = lo;
+      while (hi - lo2 > 1) { const uint32_t mid = (lo2 + hi) >> 1; if (D.rowB[mid] < end) lo2 = mid; else hi = mid; }
+      r1 = lo2 + 1;
+      r0_sh = lo;
+      nr_sh = r1 - lo;  // rows lo..r1-1 overlap the chunk (every row has an entry: <= kCompactChunk)
     }
-    if (lane == 0) {
-      D.k[s] = D.kB[s];
-      if (D.gid) D.gid[s] = D.gidB[s];
+    __syncthreads();
+    const uint32_t r0 = r0_sh, nr = nr_sh;
+    for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) rs[i] = D.rowB[r0 + i];
+    __syncthreads();
+    for (uint32_t p = start + threadIdx.x; p < end; p += blockDim.x) {
+      uint32_t lo = 0, hi = nr;  // rs[lo] <= p < rs[lo + 1]
+      while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (rs[mid] <= p) lo = mid; else hi = mid; }
+      const uint32_t src = (uint32_t)D.cd[r0 + lo] + (p - rs[lo]);
+      D.col[p] = D.colB[src];
+      wout[p] = win[src];
     }
+    __syncthreads();
+  }
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n2; s += gridDim.x * blockDim.x) {
+    D.k[s] = D.kB[s];
+    if (D.gid) D.gid[s] = D.gidB[s];
   }
 }
 
