@@ -244,8 +244,6 @@ class Run {
     int occ = 0;
     LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, false>, 512, bsmem));
     grid_block[0] = ctx->sms * std::max(1, occ);
-    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, true>, 512, 0));
-    grid_block[1] = ctx->sms * std::max(1, occ);
   }
 
   // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
@@ -287,6 +285,7 @@ class Run {
     D.hubtab = dalloc<uint32_t>(ctx, owned, n);
     D.hubself = dalloc<unsigned long long>(ctx, owned, n);
     D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
+    D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
     D.movers = dalloc<uint32_t>(ctx, owned,n);
     D.gs = dalloc<GraphState>(ctx, owned,G);
     D.ctrl = dalloc<Ctrl>(ctx, owned,1);
@@ -458,13 +457,17 @@ class Run {
     k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
     k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
-    k_opt_block<WI, true><<<grid_block[1], 512, 0, st>>>(D, 7, 0);
+    // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
+    k_opt_hub_prep<<<ctx->sms * 4, 256, 0, st>>>(D);
+    k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
+    k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
+    k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(D);
     LV_CUDA(cudaEventRecord(ev[5], st));
     k_apply<WI><<<grid_n, 256, 0, st>>>(D);
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(D);
     commit_sq();
     finalize(0);
-    launches += 14;
+    launches += 17;
   }
 
   // Runs one pass; returns the number of graphs still iterating.

@@ -34,6 +34,7 @@ struct Dev {
   uint32_t* hubtab;     // [n] aggregation: arena offset of each bin-7 new community, else kEmpty
   unsigned long long* hubself;  // [n] aggregation: self-loop weight of each bin-7 community
   unsigned long long* long_items;  // [n + E/kHubPiece + 16] (vertex << 32 | piece) of long rows
+  unsigned long long* apply_items; // [n + E/kHubPiece + 16] (mover << 32 | piece) of hub movers
   uint32_t* movers;     // [n]
   uint32_t* arena_keys;
   void* arena_vals;     // 8 bytes per slot
@@ -69,6 +70,13 @@ constexpr uint32_t kHubLongRow = 2048;
 constexpr uint32_t kHubPiece = 8192;
 
 constexpr int kMaxPartials = 2048;
+
+// Capacity of a bin-7 vertex's global optimisation table: table_cap rounded up to a whole
+// kHubChunk, so every chunk of the arena belongs to one vertex.
+__device__ __forceinline__ uint32_t hub_table_cap(uint32_t d, uint32_t ng) {
+  const uint32_t c = table_cap(d, ng);
+  return c < kHubChunk ? kHubChunk : c;
+}
 
 __device__ __forceinline__ int bin_of(const BinCfg& B, uint32_t d) {
 #pragma unroll
@@ -154,8 +162,20 @@ __global__ void k_bin_vertices(Dev D, BinCfg B) {
       const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
       if (pos != kEmpty) {
         D.bins[b][pos] = v;
-        if (b == kNumBins - 1 && want_off)
-          D.hub_off[pos] = atomicAdd(&C->hub_cursor, cap);
+        if (b == kNumBins - 1) {
+          // the row is cut into pieces for separate blocks; the table (table passes only) is a
+          // whole number of kHubChunk-slot chunks, each chunk recording its owner
+          if (want_off) {
+            const uint32_t hc = cap < kHubChunk ? kHubChunk : cap;
+            const uint32_t off = atomicAdd(&C->hub_cursor, hc);
+            D.hub_off[pos] = off;
+            if ((unsigned long long)off + hc <= C->arena_slots)
+              for (uint32_t j = 0; j < hc / kHubChunk; ++j) D.hub_owner[off / kHubChunk + j] = pos;
+          }
+          const uint32_t np = (d + kHubPiece - 1) / kHubPiece;
+          const uint32_t p0 = atomicAdd(&C->hub_items, np);
+          for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)pos << 32) | k;
+        }
       }
     }
     // pass accounting for the roofline: active vertices and their entries
@@ -185,6 +205,19 @@ __device__ __forceinline__ void emit_move(const Dev& D, bool move, uint32_t v, u
   }
 }
 
+// A mover found by a block kernel: recorded in the hub part of the mover list, its row cut into
+// pieces of kHubPiece entries for k_apply_hub.
+__device__ __forceinline__ void emit_hub_move(const Dev& D, uint32_t v, uint32_t c, uint32_t it,
+                                              uint32_t d) {
+  Ctrl* C = D.ctrl;
+  D.new_comm[v] = c;
+  D.moved_it[v] = it;
+  D.movers[C->n - 1u - atomicAdd(&C->hub_mover_count, 1u)] = v;
+  const uint32_t np = (d + kHubPiece - 1) / kHubPiece;
+  const uint32_t p0 = atomicAdd(&C->apply_items, np);
+  for (uint32_t k = 0; k < np; ++k) D.apply_items[p0 + k] = ((unsigned long long)v << 32) | k;
+}
+
 struct VtxCtx {
   uint32_t rs, re, cv, ng;  // ng: vertices of v's graph at this level
   double kv, a_own, m, two_m2;
@@ -203,6 +236,116 @@ __device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
   x.two_m2 = st.two_m2;
   x.ng = D.gid ? st.ve - st.vb : D.ctrl->n;
   return x;
+}
+
+// ---- entry loops shared by the optimisation kernels -----------------------------------------------
+// Each lane walks entries e0, e0+step, ... of the vertex in groups of kBatch: it issues the
+// group's independent loads (destinations, then their communities / totals) before using any,
+// so a lane keeps kBatch gathers in flight instead of one dependent chain per entry.
+constexpr int kBatch = 4;
+
+// Fast pass: best key over positive per-entry gains (self = 0, destination's own total).
+template <bool WINT>
+__device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxCtx& x, uint32_t v,
+                                                        uint32_t e0, uint32_t step) {
+  using Tr = WTraits<WINT>;
+  using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  unsigned long long best = 0;
+  for (uint32_t e = e0; e < x.re; e += kBatch * step) {
+    uint32_t uu[kBatch];
+    float wf[kBatch];
+    double au[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ek = e + k * step;
+      const bool in = ek < x.re;
+      uu[k] = in ? D.col[ek] : v;
+      wf[k] = in ? Tr::w_float(w[ek]) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) au[k] = uu[k] != v ? D.a[uu[k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (uu[k] == v) continue;
+      const float g = gain_ref(wf[k], 0.0f, x.kv, x.a_own, au[k], x.m, x.two_m2);
+      if (g > 0.0f) {
+        const unsigned long long key = argmax_key(g, uu[k], true);
+        best = key > best ? key : best;
+      }
+    }
+  }
+  return best;
+}
+
+// Table pass, insert half: non-loop entries into the table by destination community, the
+// vertex's own community summed into self_acc.
+template <bool WINT>
+__device__ __forceinline__ void insert_scan(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t e0,
+                                            uint32_t step, uint32_t* keys,
+                                            typename WTraits<WINT>::Acc* vals, uint32_t mask,
+                                            uint32_t shift, typename WTraits<WINT>::Acc& self_acc,
+                                            uint32_t& err) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  for (uint32_t e = e0; e < x.re; e += kBatch * step) {
+    uint32_t uu[kBatch], cc[kBatch];
+    Acc ww[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ek = e + k * step;
+      const bool in = ek < x.re;
+      uu[k] = in ? D.col[ek] : v;
+      ww[k] = in ? (Acc)w[ek] : Acc(0);
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (cc[k] == kEmpty) continue;
+      if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
+      if (!table_add(keys, vals, mask, shift, cc[k], ww[k])) err |= kErrTableFull;
+    }
+  }
+}
+
+// Table pass, evaluation half: best key over the table's communities (slots s0, s0+step, ...).
+template <bool WINT>
+__device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxCtx& x,
+                                                        const uint32_t* keys,
+                                                        const typename WTraits<WINT>::Acc* vals,
+                                                        uint32_t s0, uint32_t cap, uint32_t step,
+                                                        float self_v, bool lowest) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  unsigned long long best = 0;
+  for (uint32_t s = s0; s < cap; s += kBatch * step) {
+    uint32_t cc[kBatch];
+    Acc vv[kBatch];
+    double ac[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t sk = s + k * step;
+      const bool in = sk < cap;
+      cc[k] = in ? keys[sk] : kEmpty;
+      vv[k] = in ? vals[sk] : Acc(0);
+      if (cc[k] == x.cv) cc[k] = kEmpty;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (cc[k] == kEmpty) continue;
+      const float g = gain_ref(Tr::to_float(vv[k]), self_v, x.kv, x.a_own, ac[k], x.m, x.two_m2);
+      if (g > 0.0f) {
+        const unsigned long long key = argmax_key(g, cc[k], lowest);
+        best = key > best ? key : best;
+      }
+    }
+  }
+  return best;
 }
 
 // ---- pass: optimisation, one team of T lanes per vertex -----------------------------------------
@@ -232,7 +375,6 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
   const uint32_t it = C->it;
   const bool fast = C->fast != 0;
   const bool lowest = fast || C->rule_sort != 0;
-  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   uint32_t err = 0;
 
   for (uint32_t base = blockIdx.x * TEAMS; base < count; base += gridDim.x * TEAMS) {
@@ -243,17 +385,7 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
     if (live) x = load_vtx(D, v);
     unsigned long long best = 0;
     if (fast) {
-      if (live) {
-        for (uint32_t e = x.rs + lane; e < x.re; e += T) {
-          const uint32_t u = D.col[e];
-          if (u == v) continue;
-          const float g = gain_ref(Tr::w_float(w[e]), 0.0f, x.kv, x.a_own, D.a[u], x.m, x.two_m2);
-          if (g > 0.0f) {
-            const unsigned long long key = argmax_key(g, u, true);
-            best = key > best ? key : best;
-          }
-        }
-      }
+      if (live) best = fast_scan<WINT>(D, x, v, x.rs + lane, T);
       best = team_max<T>(best, kFull);
     } else {
       const uint32_t cap_v = live ? table_cap(x.re - x.rs, x.ng) : 2u;
@@ -263,29 +395,10 @@ __global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) 
       __syncwarp();
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
-      if (live) {
-        for (uint32_t e = x.rs + lane; e < x.re; e += T) {
-          const uint32_t u = D.col[e];
-          if (u == v) continue;
-          const uint32_t cu = D.comm[u];
-          if (cu == x.cv) { self_acc += (Acc)w[e]; continue; }
-          if (!table_add(keys, vals, mask, shift, cu, (Acc)w[e])) err |= kErrTableFull;
-        }
-      }
+      if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, keys, vals, mask, shift, self_acc, err);
       self_acc = team_sum<T>(self_acc);
       __syncwarp();
-      if (live) {
-        const float self_v = Tr::to_float(self_acc);
-        for (uint32_t s = lane; s < cap_v; s += T) {
-          const uint32_t c = keys[s];
-          if (c == kEmpty || c == x.cv) continue;
-          const float g = gain_ref(Tr::to_float(vals[s]), self_v, x.kv, x.a_own, D.a[c], x.m, x.two_m2);
-          if (g > 0.0f) {
-            const unsigned long long key = argmax_key(g, c, lowest);
-            best = key > best ? key : best;
-          }
-        }
-      }
+      if (live) best = cand_scan<WINT>(D, x, keys, vals, lane, cap_v, T, Tr::to_float(self_acc), lowest);
       best = team_max<T>(best, kFull);
       __syncwarp();
     }
@@ -355,7 +468,6 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
   const uint32_t it = C->it;
   const bool fast = C->fast != 0;
   const bool lowest = fast || C->rule_sort != 0;
-  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   uint32_t err = 0;
 
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
@@ -363,15 +475,7 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
     const VtxCtx x = load_vtx(D, v);
     unsigned long long best = 0;
     if (fast) {
-      for (uint32_t e = x.rs + threadIdx.x; e < x.re; e += NT) {
-        const uint32_t u = D.col[e];
-        if (u == v) continue;
-        const float g = gain_ref(Tr::w_float(w[e]), 0.0f, x.kv, x.a_own, D.a[u], x.m, x.two_m2);
-        if (g > 0.0f) {
-          const unsigned long long key = argmax_key(g, u, true);
-          best = key > best ? key : best;
-        }
-      }
+      best = fast_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT);
     } else {
       const uint32_t cap_v = table_cap(x.re - x.rs, x.ng);
       const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
@@ -393,41 +497,121 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
         for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
       __syncthreads();
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
-      if (ok) {
-        for (uint32_t e = x.rs + threadIdx.x; e < x.re; e += NT) {
-          const uint32_t u = D.col[e];
-          if (u == v) continue;
-          const uint32_t cu = D.comm[u];
-          if (cu == x.cv) { self_acc += (Acc)w[e]; continue; }
-          if (!table_add(keys, vals, mask, shift, cu, (Acc)w[e])) err |= kErrTableFull;
-        }
-      }
+      if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, keys, vals, mask, shift, self_acc, err);
       self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
-      if (ok) {
-        const float self_v = Tr::to_float(self_acc);
-        for (uint32_t s = threadIdx.x; s < cap_v; s += NT) {
-          const uint32_t c = keys[s];
-          if (c == kEmpty || c == x.cv) continue;
-          const float g = gain_ref(Tr::to_float(vals[s]), self_v, x.kv, x.a_own, D.a[c], x.m, x.two_m2);
-          if (g > 0.0f) {
-            const unsigned long long key = argmax_key(g, c, lowest);
-            best = key > best ? key : best;
-          }
-        }
-      }
+      if (ok) best = cand_scan<WINT>(D, x, keys, vals, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
     }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best) {
       const uint32_t c = key_comm(best, lowest);
-      if (c != x.cv && (!fast || v <= c)) {
-        D.new_comm[v] = c;
-        D.moved_it[v] = it;
-        D.movers[C->n - 1u - atomicAdd(&C->hub_mover_count, 1u)] = v;
-      }
+      if (c != x.cv && (!fast || v <= c)) emit_hub_move(D, v, c, it, x.re - x.rs);
     }
     __syncthreads();
   }
   if (err) atomicOr(&C->err, err);
+}
+
+// ---- pass: optimisation of the longest rows (bin 7), many blocks per vertex ------------------------
+// Each bin-7 row is cut into pieces of kHubPiece entries (k_bin_vertices listed them in
+// long_items); pieces are scanned by separate blocks into the vertex's global table, the table is
+// evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
+// atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
+__global__ void k_opt_hub_prep(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[kNumBins - 1];
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < count; i += nth) {
+    D.map[i] = 0ull;
+    D.hubself[i] = 0ull;
+  }
+  if (!C->fast) {
+    const uint32_t slots = min(C->hub_cursor, C->arena_slots);
+    unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
+    for (uint32_t s = tid; s < slots; s += nth) {
+      D.arena_keys[s] = kEmpty;
+      vals[s] = 0ull;
+    }
+  }
+}
+
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_opt_hub_scan(Dev D) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  __shared__ unsigned long long red[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->hub_items;
+  const bool fast = C->fast != 0;
+  uint32_t err = 0;
+  for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+    const unsigned long long item = D.long_items[i];
+    const uint32_t pos = (uint32_t)(item >> 32), piece = (uint32_t)item;
+    const uint32_t v = D.bins[kNumBins - 1][pos];
+    VtxCtx x = load_vtx(D, v);
+    const uint32_t d = x.re - x.rs;
+    const uint32_t pstart = x.rs + piece * kHubPiece;
+    x.re = min(x.re, pstart + kHubPiece);
+    if (fast) {
+      unsigned long long best = fast_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x);
+      best = block_max<256>(best, red);
+      if (threadIdx.x == 0 && best) atomicMax(&D.map[pos], best);
+    } else {
+      const uint32_t cap = hub_table_cap(d, x.ng);
+      const uint32_t off = D.hub_off[pos];
+      const bool ok = (unsigned long long)off + cap <= C->arena_slots;
+      if (!ok) err |= kErrArena;
+      Acc self_acc = Acc(0);
+      if (ok)
+        insert_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x, D.arena_keys + off,
+                          reinterpret_cast<Acc*>(D.arena_vals) + off, cap - 1u,
+                          32u - log2_pow2(cap), self_acc, err);
+      self_acc = block_sum<256>(self_acc, reinterpret_cast<Acc*>(red));
+      if (threadIdx.x == 0 && self_acc != Acc(0)) {
+        if (WINT) atomicAdd(&D.hubself[pos], (unsigned long long)self_acc);
+        else atomicAdd(reinterpret_cast<double*>(&D.hubself[pos]), (double)self_acc);
+      }
+    }
+  }
+  if (err) atomicOr(&C->err, err);
+}
+
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_opt_hub_eval(Dev D) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  __shared__ unsigned long long red[33];
+  Ctrl* C = D.ctrl;
+  if (C->fast) return;
+  const bool lowest = C->rule_sort != 0;
+  const uint32_t nchunks = min(C->hub_cursor, C->arena_slots) / kHubChunk;
+  const Acc* vals = reinterpret_cast<const Acc*>(D.arena_vals);
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const uint32_t pos = D.hub_owner[c];
+    const uint32_t v = D.bins[kNumBins - 1][pos];
+    const VtxCtx x = load_vtx(D, v);
+    const unsigned long long hs = D.hubself[pos];
+    float self_v;
+    if (WINT) self_v = Tr::to_float((Acc)hs);
+    else self_v = Tr::to_float((Acc)__longlong_as_double((long long)hs));
+    unsigned long long best = cand_scan<WINT>(D, x, D.arena_keys, vals, c * kHubChunk + threadIdx.x,
+                                              (c + 1) * kHubChunk, blockDim.x, self_v, lowest);
+    best = block_max<256>(best, red);
+    if (threadIdx.x == 0 && best) atomicMax(&D.map[pos], best);
+  }
+}
+
+__global__ void k_opt_hub_decide(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[kNumBins - 1], it = C->it;
+  const bool fast = C->fast != 0;
+  const bool lowest = fast || C->rule_sort != 0;
+  for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < count; pos += gridDim.x * blockDim.x) {
+    const unsigned long long best = D.map[pos];
+    if (!best) continue;
+    const uint32_t v = D.bins[kNumBins - 1][pos];
+    const uint32_t c = key_comm(best, lowest);
+    if (c != D.comm[v] && (!fast || v <= c)) emit_hub_move(D, v, c, it, D.row[v + 1] - D.row[v]);
+  }
 }
 
 // ---- pass: apply the moves, propagate activity, update the internal weight ---------------------
@@ -448,17 +632,33 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
   using Tr = WTraits<WINT>;
   using Wt = typename Tr::W;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
-  for (uint32_t e = e0; e < re; e += step) {
-    const uint32_t u = D.col[e];
-    const uint32_t pre = D.comm[u];
-    const bool mu = D.moved_it[u] == it;
-    const uint32_t post = mu ? D.new_comm[u] : pre;
-    if (post != nw) D.active_it[u] = it + 1;
-    const int dd = (int)(nw == post) - (int)(old == pre);
-    if (dd) {
-      const int f = mu ? dd : 2 * dd;
-      if (WINT) di += (long long)f * (long long)w[e];
-      else df += (double)f * Tr::w_double(w[e]);
+  // kBatch entries per lane at a time: their gathers are issued before any is used
+  for (uint32_t e = e0; e < re; e += kBatch * step) {
+    uint32_t uu[kBatch], pre[kBatch], mv[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ek = e + k * step;
+      uu[k] = ek < re ? D.col[ek] : kEmpty;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      pre[k] = uu[k] != kEmpty ? D.comm[uu[k]] : 0u;
+      mv[k] = uu[k] != kEmpty ? D.moved_it[uu[k]] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (uu[k] == kEmpty) continue;
+      const uint32_t u = uu[k];
+      const bool mu = mv[k] == it;
+      const uint32_t post = mu ? D.new_comm[u] : pre[k];
+      if (post != nw) D.active_it[u] = it + 1;
+      const int dd = (int)(nw == post) - (int)(old == pre[k]);
+      if (dd) {
+        const uint32_t ek = e + k * step;
+        const int f = mu ? dd : 2 * dd;
+        if (WINT) di += (long long)f * (long long)w[ek];
+        else df += (double)f * Tr::w_double(w[ek]);
+      }
     }
   }
 }
@@ -493,26 +693,30 @@ __global__ void __launch_bounds__(256) k_apply(Dev D) {
   }
 }
 
-// One block per mover found by the block kernels (vertices with long rows).
+// Movers found by the block kernels (vertices with long rows): one block per piece of
+// kHubPiece entries of their rows; the first piece also moves the totals.
 template <bool WINT>
 __global__ void __launch_bounds__(512) k_apply_hub(Dev D) {
   Ctrl* C = D.ctrl;
-  const uint32_t count = C->hub_mover_count, it = C->it, n = C->n;
+  const uint32_t count = C->apply_items, it = C->it;
   __shared__ long long shi[32];
   __shared__ double shf[32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
-    const uint32_t v = D.movers[n - 1u - idx];
+    const unsigned long long item = D.apply_items[idx];
+    const uint32_t v = (uint32_t)(item >> 32), piece = (uint32_t)item;
     const uint32_t old = D.comm[v], nw = D.new_comm[v];
     const uint32_t g = D.gid ? D.gid[v] : 0u;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && piece == 0) {
       const double kv = D.k[v];
       atomicAdd(&D.a[nw], kv);
       atomicAdd(&D.a[old], -kv);
     }
     long long di = 0;
     double df = 0.0;
-    apply_entries<WINT>(D, v, old, nw, it, D.row[v] + threadIdx.x, D.row[v + 1], blockDim.x, di, df);
+    const uint32_t ps = D.row[v] + piece * kHubPiece;
+    const uint32_t pe = min(D.row[v + 1], ps + kHubPiece);
+    apply_entries<WINT>(D, v, old, nw, it, ps + threadIdx.x, pe, blockDim.x, di, df);
     di = warp_sum(di);
     df = warp_sum(df);
     if (lane == 0) { shi[wid] = di; shf[wid] = df; }
@@ -676,6 +880,8 @@ __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->mover_count = 0;
     C->hub_mover_count = 0;
+    C->hub_items = 0;
+    C->apply_items = 0;
     C->hub_cursor = 0;
     for (uint32_t i = 0; i < C->n_chunks && i < kMaxChunks; ++i) C->chunk_any[i] = 0;
     C->act_entries_total += C->act_entries;
@@ -710,6 +916,8 @@ __global__ void k_level_init(Dev D) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->mover_count = 0;
     C->hub_mover_count = 0;
+    C->hub_items = 0;
+    C->apply_items = 0;
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
     for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
@@ -927,8 +1135,8 @@ __global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap, unsign
     const uint32_t d = D.row[v + 1] - D.row[v];
     if (d <= min_deg) continue;
     const uint32_t g = D.gid ? D.gid[v] : 0u;
-    const uint32_t cap = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
-    if (cap > block_cap) s += cap;
+    const uint32_t ng = D.gid ? D.gs[g].ve - D.gs[g].vb : n;
+    if (table_cap(d, ng) > block_cap) s += hub_table_cap(d, ng);
   }
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(need, s);
