@@ -28,12 +28,19 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "louvain-fast-move-cuda_b200"
 
 SCALE, EDGE_FACTOR, SEED = 22, 16, 1
 WORKLOAD = "rmat_s22_ef16"
+# DRAM bytes (read + write, ncu dram__bytes_*) of the optimisation kernels over one run divided
+# by their algorithmic bytes, from an ncu capture of one scale-20 run of the same generator
+# (2.791 GB of DRAM traffic for 2.204 GB algorithmic); the scale-22 traffic is that ratio times
+# its own algorithmic bytes.
+OPT_TRAFFIC_RATIO = 2.791 / 2.204
 
 
 def parse():
@@ -46,6 +53,16 @@ def parse():
     ap.add_argument("--mode", default="SORT", choices=["SORT", "HASH"])
     ap.add_argument("--cpu-sample-scale", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--once", action="store_true",
+                    help="one untimed run on the device-resident graph (for profilers), then exit")
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batched", "served"],
+                    help="rmat: the single R-MAT graph (default line); batched: 4,096 uneven "
+                         "Chung-Lu graphs in one batch against a loop of single runs; served: "
+                         "Poisson request stream through the server against a loop")
+    ap.add_argument("--graphs", type=int, default=4096, help="batched: number of graphs")
+    ap.add_argument("--pool", type=int, default=64, help="served: distinct request graphs")
+    ap.add_argument("--slots", type=int, default=16, help="served: concurrent server slots")
+    ap.add_argument("--rates", default="10,50,200,1000,2000", help="served: arrival rates, req/s")
     return ap.parse_args()
 
 
@@ -69,6 +86,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.t0 = 0.0
 
     def __enter__(self):
         try:
@@ -84,7 +102,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self):
+        """Start of the window whose samples summary() reports."""
+        self.t0 = time.perf_counter()
 
     def __exit__(self, *a):
         if self.proc:
@@ -97,7 +119,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0 = getattr(self, "t0", 0.0)
+        for t, ln in self.lines:
+            if t < t0:
+                continue
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -203,6 +228,163 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_batched(args, local):
+    """4,096 Chung-Lu graphs (exponent 2.1, mean degree 8, n log-uniform in [200, 200,000])
+    in one lv_run_batch call, against the same graphs run one lv_run_csr call at a time."""
+    import importlib
+    import torch
+    lv = importlib.import_module(PKG)
+    graphs = importlib.import_module(PKG + ".graphs")
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    b = graphs.chung_lu_batch_device(G=args.graphs, seed=SEED, device=dev)
+    mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
+    eng = lv.Engine(local, mode=mode)
+    N = int(b.n.sum())
+    out_d = torch.empty(N, dtype=torch.int32, device=dev)
+    for _ in range(max(1, args.warmup)):
+        eng.run_batch(b.vtx_offsets, b.row_ptr, b.col, out=out_d)
+    torch.cuda.synchronize()
+    ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            _, qs, ks, st = eng.run_batch(b.vtx_offsets, b.row_ptr, b.col, out=out_d)
+            ms.append(st.ms_total)
+    batch_ms = sum(ms) / len(ms)
+    launches = st.kernel_launches
+
+    # the baseline: one single-graph call per graph on the same device-resident data
+    singles = [b.graph(g) for g in range(b.G)]
+    outs = [torch.empty(n, dtype=torch.int32, device=dev) for n, _, _ in singles]
+    for g in range(min(8, b.G)):
+        eng.run_csr(singles[g][0], singles[g][1], singles[g][2], None, out=outs[g])
+    torch.cuda.synchronize()
+    q_loop = np.empty(b.G)
+    t0 = time.perf_counter()
+    loop_launches = 0
+    for g, (n, rp, col) in enumerate(singles):
+        _, q_loop[g], s1 = eng.run_csr(n, rp, col, None, out=outs[g])
+        loop_launches += s1.kernel_launches
+    torch.cuda.synchronize()
+    loop_ms = (time.perf_counter() - t0) * 1e3
+    offs = b.vtx_offsets.cpu().numpy()
+    same = all(torch.equal(out_d[offs[g]: offs[g + 1]], outs[g]) for g in range(b.G))
+    m_total = int(b.m.sum())
+    line = {
+        "metric": "batched_graphs_per_s", "value": b.G / (batch_ms / 1e3), "unit": "graphs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": batch_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 weights, f32 gains, f64 totals", "data": "synthetic",
+        "config": {"workload": f"chung_lu_batch_G{b.G}_n200-200000_g2.1_k8", "graphs": b.G,
+                   "n_total": N, "m_total": m_total, "mode": args.mode, "threshold": 1e-3,
+                   "l2": "inputs larger than L2 (packed CSR %.2f GB)" % ((2 * m_total * 4 + 8 * N) / 1e9)},
+        "edges_per_s": m_total / (batch_ms / 1e3),
+        "loop": {"graphs_per_s": b.G / (loop_ms / 1e3), "ms": loop_ms, "gpu_launches": int(loop_launches),
+                 "what": "one lv_run_csr call per graph, device-resident inputs, same engine"},
+        "speedup_vs_loop": loop_ms / batch_ms,
+        "parity": {"partitions_equal": bool(same),
+                   "max_abs_dq": float(np.max(np.abs(np.asarray(qs) - q_loop)))},
+        "levels": st.levels, "passes": st.iterations, "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
+def _percentile(xs, p):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(p / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def run_served(args, local):
+    """Poisson arrivals of R-MAT requests (edge factor 8, n log-uniform in [1,000, 2,000,000])
+    into the server (150 GB budget, `slots` concurrent streams), swept over arrival rates,
+    against the same requests run one lv_run_csr call at a time from the same host buffers."""
+    import importlib
+    import torch
+    lv = importlib.import_module(PKG)
+    graphs = importlib.import_module(PKG + ".graphs")
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(SEED)
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(2_000_000), args.pool)).astype(np.int64)
+    pool, keep = [], []
+    for i, nt in enumerate(sizes):
+        g = graphs.rmat_device(int(nt), 8, seed=SEED + i, device=dev)
+        rp = torch.from_numpy(g.row_ptr).pin_memory()
+        cl = torch.from_numpy(g.col).pin_memory()
+        keep.append((rp, cl))
+        pool.append(graphs.CSRGraph(n=g.n, row_ptr=rp.numpy(), col=cl.numpy(), w=None, name=g.name))
+    torch.cuda.empty_cache()
+    eng = lv.Engine(local)
+    # loop baseline: the pool once, one call per request, host buffers in and out
+    for g in pool[:4]:
+        eng.run_graph(g)
+    ref_q = []
+    t0 = time.perf_counter()
+    for g in pool:
+        ref_q.append(eng.run_graph(g)[1])
+    loop_s = time.perf_counter() - t0
+    loop_gps = len(pool) / loop_s
+
+    srv = lv.Server(eng, 150 << 30, slots=args.slots)
+    for g in pool[:args.slots]:
+        srv.submit(g, borrow=True)
+    srv.drain()
+    rates = []
+    worst_dq = 0.0
+    with ClockSampler(local) as clk:
+        for rate in [float(x) for x in args.rates.split(",")]:
+            n_req = int(min(400, max(24, rate * 2.0)))
+            gaps = rng.exponential(1.0 / rate, n_req)
+            which = rng.integers(0, len(pool), n_req)
+            ids, lat = {}, []
+            t_start = time.perf_counter()
+            t_next = t_start
+            i = 0
+            done_t = None
+            while i < n_req or ids:
+                now = time.perf_counter()
+                while i < n_req and now >= t_next:
+                    ids[srv.submit(pool[which[i]], borrow=True)] = which[i]
+                    t_next += gaps[i]
+                    i += 1
+                for rid in list(ids):
+                    r = srv.poll(rid)
+                    if r is not None:
+                        lat.append(r[2])
+                        worst_dq = max(worst_dq, abs(r[1] - ref_q[ids.pop(rid)]))
+                        done_t = time.perf_counter()
+                time.sleep(0.0002)
+            span = done_t - t_start
+            rates.append({"rate": rate, "requests": n_req, "graphs_per_s": n_req / span,
+                          "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99)})
+    best = max(rates, key=lambda r: r["graphs_per_s"])
+    line = {
+        "metric": "served_graphs_per_s", "value": best["graphs_per_s"], "unit": "graphs/s",
+        "n_gpus": 1, "steps": len(rates), "warmup": 1, "ms_per_step": 1e3 / best["graphs_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 weights, f32 gains, f64 totals", "data": "synthetic",
+        "config": {"workload": "rmat_ef8_n1000-2000000_poisson", "pool": len(pool),
+                   "mean_m": float(np.mean([g.m for g in pool])), "slots": args.slots,
+                   "budget_gb": 150, "mode": "SORT"},
+        "rates": rates, "p50_ms_at_best": best["p50_ms"], "p99_ms_at_best": best["p99_ms"],
+        "loop": {"graphs_per_s": loop_gps, "what": "the pool once, one lv_run_csr call per "
+                                                    "request from the same pinned host buffers"},
+        "speedup_vs_loop": best["graphs_per_s"] / loop_gps,
+        "parity": {"max_abs_dq_vs_alone": worst_dq},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    srv.close()
+    eng.close()
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
@@ -212,6 +394,10 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return rc
+    if args.workload == "batched":
+        return run_batched(args, local) if rank == 0 else 0
+    if args.workload == "served":
+        return run_served(args, local) if rank == 0 else 0
 
     import importlib
     import torch
@@ -225,33 +411,41 @@ def main():
     row_d = torch.from_numpy(g.row_ptr).to(dev)
     col_d = torch.from_numpy(g.col).to(dev)
     out_d = torch.empty(g.n, dtype=torch.int32, device=dev)
+    if args.once:
+        _, q, st = eng.run_csr(g.n, row_d, col_d, None, out=out_d)
+        if rank == 0:
+            print(json.dumps({"once": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "modularity": q,
+                              "passes": st.iterations, "levels": st.levels, "ms": st.ms_total,
+                              "bytes_optimization": st.bytes_optimization,
+                              "ms_optimization_kernels": st.ms_optimization_kernels,
+                              "kernel_launches": st.kernel_launches}), flush=True)
+        eng.close()
+        return 0
     row_h = torch.from_numpy(g.row_ptr).pin_memory()
     col_h = torch.from_numpy(g.col).pin_memory()
     out_h = torch.empty(g.n, dtype=torch.int32).pin_memory()
     row_h_np, col_h_np, out_h_np = row_h.numpy(), col_h.numpy(), out_h.numpy()
 
+    # clocks are sampled from the first timed run to the last end-to-end run (the sampler
+    # starts before the warm-up so that it is running when the timed region begins)
+    clk = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         eng.run_csr(g.n, row_d, col_d, None, out=out_d)
     torch.cuda.synchronize()
 
     # device-resident runs (value)
     stats = []
-    with ClockSampler(local) as clk:
-        barrier(world)
-        torch.cuda.synchronize()
-        s_ev = torch.cuda.Event(enable_timing=True)
-        e_ev = torch.cuda.Event(enable_timing=True)
-        s_ev.record()
-        wall0 = time.perf_counter()
-        for _ in range(args.steps):
-            _, q, st = eng.run_csr(g.n, row_d, col_d, None, out=out_d)
-            stats.append(st)
-        # the engine runs on its own stream and synchronises it before returning; the torch
-        # events bracket the same region on the current stream after that synchronisation
-        e_ev.record()
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - wall0
-        barrier(world)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk.mark()
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        # the engine times each run with CUDA events on its own stream (st.ms_total)
+        _, q, st = eng.run_csr(g.n, row_d, col_d, None, out=out_d)
+        stats.append(st)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    barrier(world)
     engine_ms = sum(s.ms_total for s in stats) / len(stats)   # engine-stream CUDA events
     ms_step = max_over_ranks(engine_ms, world)
     value = world * g.m / (ms_step / 1e3)
@@ -265,6 +459,7 @@ def main():
     torch.cuda.synchronize()
     e2e_sec = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
     barrier(world)
+    clk.__exit__(None, None, None)
 
     st = stats[-1]
     peak, peak_kind = measured_peak()
@@ -286,7 +481,9 @@ def main():
                 "d2h_bytes_per_step": int(g.n * 4), "ms_per_step": e2e_sec * 1e3,
                 "modularity": q_e2e},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": st.bytes_optimization * OPT_TRAFFIC_RATIO,
+                     "traffic_source": "ncu dram__bytes_read+write of the same kernels at scale 20, "
+                                       "as a ratio to algorithmic bytes, applied to this run",
                      "kernel": "optimisation kernels (binning + gain evaluation), all passes",
                      "bytes": st.bytes_optimization, "ms": st.ms_optimization_kernels,
                      "peak_source": peak_kind},

@@ -223,9 +223,14 @@ typedef struct lv_server lv_server;
 lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_slots,
                            lv_server** out);
 lv_status lv_server_destroy(lv_server* s);
-/* Copies the request's host CSR into pinned staging memory and queues it; returns its id. */
+/* Copies the request's host CSR (the caller may reuse its buffers at once) and queues it;
+ * returns its id. */
 lv_status lv_server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, const int32_t* col,
                            const float* w, int64_t* request_id);
+/* The same without the copy: the buffers are borrowed and must stay valid and unchanged until
+ * lv_server_poll reports the request done (pinned host memory gives full-speed uploads). */
+lv_status lv_server_submit_borrowed(lv_server* s, int64_t n, const int64_t* row_ptr,
+                                    const int32_t* col, const float* w, int64_t* request_id);
 /* Moves finished work forward; returns immediately. *n_done = finished requests so far. */
 lv_status lv_server_progress(lv_server* s, int64_t* n_done, int64_t* n_inflight,
                              int64_t* n_queued);

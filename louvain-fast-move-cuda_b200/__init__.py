@@ -101,8 +101,8 @@ EXPORTS = (
     "lv_community_destroy", "lv_optimization_step", "lv_optimization_run",
     "lv_aggregation_run", "lv_louvain", "lv_community_info_get", "lv_community_get_partition",
     "lv_community_get_best", "lv_community_get_graph", "lv_community_get_trace",
-    "lv_server_create", "lv_server_destroy", "lv_server_submit", "lv_server_progress",
-    "lv_server_poll", "lv_server_drain",
+    "lv_server_create", "lv_server_destroy", "lv_server_submit", "lv_server_submit_borrowed",
+    "lv_server_progress", "lv_server_poll", "lv_server_drain",
 )
 
 
@@ -141,6 +141,7 @@ def load_library(path: Optional[str] = None):
         "lv_server_create": (i32, [vp, i64, i32, P(vp)]),
         "lv_server_destroy": (i32, [vp]),
         "lv_server_submit": (i32, [vp, i64, vp, vp, vp, P(i64)]),
+        "lv_server_submit_borrowed": (i32, [vp, i64, vp, vp, vp, P(i64)]),
         "lv_server_progress": (i32, [vp, P(i64), P(i64), P(i64)]),
         "lv_server_poll": (i32, [vp, i64, vp, P(dbl), P(dbl), P(i32)]),
         "lv_server_drain": (i32, [vp]),
@@ -349,6 +350,67 @@ class CommunityState:
         self.e.check(self.e._L.lv_community_get_trace(self._h, out.ctypes.data, cap, ctypes.byref(ln)),
                      "lv_community_get_trace")
         return out[: min(ln.value, cap)]
+
+
+class Server:
+    """lv_server_*: requests admitted under a device-memory budget into `slots` concurrent
+    streams of one Engine's device; each request is one single-graph Louvain run."""
+
+    def __init__(self, engine: Engine, budget_bytes: int, slots: int = 8):
+        self.e = engine
+        h = ctypes.c_void_p()
+        engine.check(engine._L.lv_server_create(engine._h, int(budget_bytes), int(slots), ctypes.byref(h)),
+                     "lv_server_create")
+        self._h = h
+        self.n_of = {}
+        self._held = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.e._L.lv_server_destroy(self._h)  # joins the workers: borrowed buffers are free after
+            self._h = None
+            self._held = {}
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, g: CSRGraph, borrow: bool = False) -> int:
+        """Queues host CSR `g` and returns the request id. borrow=False copies the arrays at
+        submit; borrow=True hands them to the server as they are (lv_server_submit_borrowed),
+        and this object keeps them referenced until the request is polled done."""
+        row = np.ascontiguousarray(g.row_ptr, dtype=np.int64)
+        col = np.ascontiguousarray(g.col, dtype=np.int32)
+        w = None if g.w is None else np.ascontiguousarray(g.w, dtype=np.float32)
+        rid = ctypes.c_int64(0)
+        fn = self.e._L.lv_server_submit_borrowed if borrow else self.e._L.lv_server_submit
+        self.e.check(fn(self._h, int(g.n), row.ctypes.data, col.ctypes.data,
+                        None if w is None else w.ctypes.data, ctypes.byref(rid)),
+                     "lv_server_submit")
+        self.n_of[rid.value] = int(g.n)
+        if borrow:
+            self._held[rid.value] = (row, col, w)
+        return rid.value
+
+    def progress(self):
+        """(finished, running, queued) request counts."""
+        d, r, q = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self.e.check(self.e._L.lv_server_progress(self._h, ctypes.byref(d), ctypes.byref(r), ctypes.byref(q)),
+                     "lv_server_progress")
+        return d.value, r.value, q.value
+
+    def poll(self, rid: int):
+        """None while request `rid` runs; then (communities, modularity, latency_ms)."""
+        out = np.empty(self.n_of[rid], dtype=np.int32)
+        q, lat, done = ctypes.c_double(), ctypes.c_double(), ctypes.c_int32(0)
+        st = self.e._L.lv_server_poll(self._h, int(rid), out.ctypes.data, ctypes.byref(q),
+                                      ctypes.byref(lat), ctypes.byref(done))
+        if done.value or st != 0:
+            self._held.pop(rid, None)
+        self.e.check(st, "lv_server_poll")
+        return (out, q.value, lat.value) if done.value else None
+
+    def drain(self):
+        self.e.check(self.e._L.lv_server_drain(self._h), "lv_server_drain")
 
 
 # ---- the reference's own names -------------------------------------------------------------------

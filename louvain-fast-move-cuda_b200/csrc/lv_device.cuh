@@ -63,6 +63,8 @@ struct GraphState {
   uint32_t total_iters;
   uint32_t moved;     // moves of the last pass
   uint32_t n_next;    // aggregation: vertices of this graph at the next level
+  double inv_m;       // rn(1/m) and rn(1/two_m2), for the gain upper bound only
+  double inv_2m2;
 };
 
 // Hash-table capacity for a row of d entries in a graph of ng vertices: twice the number of
@@ -121,12 +123,32 @@ struct Ctrl {
 // w_vc - self_v, then double: diff/m + k*(a_own - k - a_c)/((2m)m), rounded to float. The
 // explicit _rn intrinsics keep every step a single IEEE rounding (no FMA contraction), so the
 // result is bit-identical to the reference and to the oracle.
+// The two operands of the gain: diff = w_vc - self_v (float) and p = k*((a_own - k) - a_c).
+__device__ __forceinline__ double gain_p(double k, double own_minus_k, double a_c) {
+  return __dmul_rn(k, __dsub_rn(own_minus_k, a_c));
+}
+__device__ __forceinline__ float gain_exact(float diff, double p, double m, double two_m2) {
+  return __double2float_rn(__dadd_rn(__ddiv_rn((double)diff, m), __ddiv_rn(p, two_m2)));
+}
 __device__ __forceinline__ float gain_ref(float w_vc, float self_v, double k, double a_own,
                                           double a_c, double m, double two_m2) {
-  const float diff = __fsub_rn(w_vc, self_v);
-  const double t1 = __ddiv_rn((double)diff, m);
-  const double t2 = __ddiv_rn(__dmul_rn(k, __dsub_rn(__dsub_rn(a_own, k), a_c)), two_m2);
-  return __double2float_rn(__dadd_rn(t1, t2));
+  return gain_exact(__fsub_rn(w_vc, self_v), gain_p(k, __dsub_rn(a_own, k), a_c), m, two_m2);
+}
+
+// An upper bound of gain_exact(diff, p, m, two_m2) without division, for discarding candidates
+// that cannot beat the best gain found so far. With r1 = rn(1/m) and r2 = rn(1/two_m2),
+// t1 = rn(diff*r1) and t2 = rn(p*r2) are each within 3 units of 2^-53 (relative) of the exact
+// quotients rn(diff/m) and rn(p/two_m2) (one rounding in the reciprocal, one in the product,
+// one in the quotient), so rn(t1 + t2) is within 5 * 2^-53 * (|t1| + |t2|) of the reference's
+// double sum. err = 2^-49 * (|t1| + |t2|) + 2^-1000 covers that with room to spare (the
+// absolute term covers subnormal results); adding it rounding up and converting to float
+// rounding up gives a float >= the reference's rn-to-float gain, since both roundings are
+// monotone.
+__device__ __forceinline__ float gain_upper(float diff, double p, double inv_m, double inv_2m2) {
+  const double t1 = __dmul_rn((double)diff, inv_m);
+  const double t2 = __dmul_rn(p, inv_2m2);
+  const double err = __fma_rn(__dadd_rn(fabs(t1), fabs(t2)), 0x1p-49, 0x1p-1000);
+  return __double2float_ru(__dadd_ru(__dadd_rn(t1, t2), err));
 }
 
 // Argmax key for a positive gain: the float bits order positive floats, the low word breaks

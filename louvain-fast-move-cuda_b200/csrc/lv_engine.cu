@@ -119,6 +119,20 @@ static T* dalloc(lv_context* ctx, std::vector<Block>& owned, size_t count) {
   return reinterpret_cast<T*>(p);
 }
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the current device.
+// The limit is per process and device, and runs on several host threads (the serving loop)
+// launch the same kernels with different table sizes, so it only ever grows: lowering it for
+// one run could fail another run's launch in flight.
+static void ensure_dyn_smem(int device, const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> set;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = set[{device, fn}];
+  if (bytes <= cur) return;
+  LV_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
+
 struct HostCtrlSnap {
   uint32_t it, n, E, n0, G, n_iterating, err, fast, rule_sort;
 };
@@ -223,8 +237,8 @@ class Run {
   template <int T>
   void team_grid(int b, const void* opt_fn, const void* con_fn) {
     const size_t smem = (size_t)(256 / T) * team_cap[b] * (4 + acc_size());
-    LV_CUDA(cudaFuncSetAttribute(opt_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LV_CUDA(cudaFuncSetAttribute(con_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ensure_dyn_smem(ctx->device, opt_fn, smem);
+    ensure_dyn_smem(ctx->device, con_fn, smem);
     int occ = 0;
     LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, opt_fn, 256, smem));
     grid_team[b] = ctx->sms * std::max(1, occ);
@@ -239,8 +253,8 @@ class Run {
     team_grid<32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     const size_t bsmem = (size_t)block_cap * (4 + acc_size());
-    LV_CUDA(cudaFuncSetAttribute((const void*)k_opt_block<WI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
-    LV_CUDA(cudaFuncSetAttribute((const void*)k_contract_block<WI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI, false>, bsmem);
+    ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, bsmem);
     int occ = 0;
     LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, false>, 512, bsmem));
     grid_block[0] = ctx->sms * std::max(1, occ);

@@ -221,6 +221,7 @@ __device__ __forceinline__ void emit_hub_move(const Dev& D, uint32_t v, uint32_t
 struct VtxCtx {
   uint32_t rs, re, cv, ng;  // ng: vertices of v's graph at this level
   double kv, a_own, m, two_m2;
+  double own_minus_k, inv_m, inv_2m2;  // a_own - k (the reference's first subtraction); bounds
 };
 
 __device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
@@ -234,6 +235,9 @@ __device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
   const GraphState& st = D.gs[g];
   x.m = st.m;
   x.two_m2 = st.two_m2;
+  x.own_minus_k = __dsub_rn(x.a_own, x.kv);
+  x.inv_m = st.inv_m;
+  x.inv_2m2 = st.inv_2m2;
   x.ng = D.gid ? st.ve - st.vb : D.ctrl->n;
   return x;
 }
@@ -252,6 +256,7 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
   using Wt = typename Tr::W;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   unsigned long long best = 0;
+  float bestg = 0.0f;  // gain of `best` (0 while there is none)
   for (uint32_t e = e0; e < x.re; e += kBatch * step) {
     uint32_t uu[kBatch];
     float wf[kBatch];
@@ -268,10 +273,16 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       if (uu[k] == v) continue;
-      const float g = gain_ref(wf[k], 0.0f, x.kv, x.a_own, au[k], x.m, x.two_m2);
-      if (g > 0.0f) {
-        const unsigned long long key = argmax_key(g, uu[k], true);
-        best = key > best ? key : best;
+      // self = 0: diff = w - 0 = w exactly
+      const double p = gain_p(x.kv, x.own_minus_k, au[k]);
+      // the division-free bound discards every entry that cannot reach the best gain so far
+      const float hi = gain_upper(wf[k], p, x.inv_m, x.inv_2m2);
+      if (hi > 0.0f && hi >= bestg) {
+        const float g = gain_exact(wf[k], p, x.m, x.two_m2);
+        if (g > 0.0f) {
+          const unsigned long long key = argmax_key(g, uu[k], true);
+          if (key > best) { best = key; bestg = g; }
+        }
       }
     }
   }
@@ -321,6 +332,7 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   unsigned long long best = 0;
+  float bestg = 0.0f;  // gain of `best` (0 while there is none)
   for (uint32_t s = s0; s < cap; s += kBatch * step) {
     uint32_t cc[kBatch];
     Acc vv[kBatch];
@@ -338,10 +350,15 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       if (cc[k] == kEmpty) continue;
-      const float g = gain_ref(Tr::to_float(vv[k]), self_v, x.kv, x.a_own, ac[k], x.m, x.two_m2);
-      if (g > 0.0f) {
-        const unsigned long long key = argmax_key(g, cc[k], lowest);
-        best = key > best ? key : best;
+      const float diff = __fsub_rn(Tr::to_float(vv[k]), self_v);
+      const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
+      const float hi = gain_upper(diff, p, x.inv_m, x.inv_2m2);
+      if (hi > 0.0f && hi >= bestg) {
+        const float g = gain_exact(diff, p, x.m, x.two_m2);
+        if (g > 0.0f) {
+          const unsigned long long key = argmax_key(g, cc[k], lowest);
+          if (key > best) { best = key; bestg = g; }
+        }
       }
     }
   }
@@ -1104,6 +1121,8 @@ __global__ void k_prep_total(Dev D) {
     }
     st->m = twice / 2.0;
     st->two_m2 = __dmul_rn(__dmul_rn(2.0, st->m), st->m);
+    st->inv_m = __drcp_rn(st->m);
+    st->inv_2m2 = __drcp_rn(st->two_m2);
     st->S = 0;
   }
 }

@@ -23,6 +23,10 @@ struct Request {
   std::vector<int64_t> row;
   std::vector<int32_t> col;
   std::vector<float> w;
+  // borrowed requests: the caller's buffers, valid until the request is polled done
+  const int64_t* brow = nullptr;
+  const int32_t* bcol = nullptr;
+  const float* bw = nullptr;
   bool weighted = false;
   std::vector<int32_t> out;
   double modularity = 0;
@@ -94,8 +98,9 @@ struct lv_server {
   void run_one(lv::Request* r, int slot) {
     try {
       lv::Run run(ctx, streams[slot]);
-      run.init(1, nullptr, r->n, r->row.data(), r->col.data(), r->weighted ? r->w.data() : nullptr,
-               LV_MEM_HOST);
+      const bool borrowed = r->brow != nullptr;
+      run.init(1, nullptr, r->n, borrowed ? r->brow : r->row.data(), borrowed ? r->bcol : r->col.data(),
+               r->weighted ? (borrowed ? r->bw : r->w.data()) : nullptr, LV_MEM_HOST);
       run.louvain();
       r->out.resize((size_t)r->n);
       lv::GraphState gs;
@@ -162,8 +167,8 @@ lv_status lv_server_destroy(lv_server* s) {
   return LV_OK;
 }
 
-lv_status lv_server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, const int32_t* col,
-                           const float* w, int64_t* request_id) {
+static lv_status server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                               const float* w, bool borrow, int64_t* request_id) {
   if (!s || !row_ptr || !col || !request_id || n <= 0) return LV_ERR_ARGUMENT;
   const int64_t E = row_ptr[n];
   if (E <= 0 || E > (1ll << 30)) return LV_ERR_RANGE;
@@ -172,13 +177,17 @@ lv_status lv_server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, cons
   r->E = E;
   r->est_bytes = lv::footprint(n, E);
   if ((int64_t)r->est_bytes > s->budget) return LV_ERR_BUDGET;
-  r->row.assign(row_ptr, row_ptr + n + 1);
-  r->col.assign(col, col + E);
-  if (w) {
-    r->weighted = true;
-    r->w.assign(w, w + E);
-  }
   r->t_submit = std::chrono::steady_clock::now();
+  r->weighted = w != nullptr;
+  if (borrow) {
+    r->brow = row_ptr;
+    r->bcol = col;
+    r->bw = w;
+  } else {
+    r->row.assign(row_ptr, row_ptr + n + 1);
+    r->col.assign(col, col + E);
+    if (w) r->w.assign(w, w + E);
+  }
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return LV_ERR_STATE;
@@ -189,6 +198,16 @@ lv_status lv_server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, cons
   }
   s->cv_work.notify_all();
   return LV_OK;
+}
+
+lv_status lv_server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                           const float* w, int64_t* request_id) {
+  return server_submit(s, n, row_ptr, col, w, false, request_id);
+}
+
+lv_status lv_server_submit_borrowed(lv_server* s, int64_t n, const int64_t* row_ptr,
+                                    const int32_t* col, const float* w, int64_t* request_id) {
+  return server_submit(s, n, row_ptr, col, w, true, request_id);
 }
 
 lv_status lv_server_progress(lv_server* s, int64_t* n_done, int64_t* n_inflight, int64_t* n_queued) {

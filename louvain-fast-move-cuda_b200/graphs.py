@@ -268,3 +268,145 @@ def to_device_canonical(u, v, device="cuda", name: str = "") -> CSRGraph:
     row_ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
     row_ptr[1:] = torch.cumsum(counts, 0)
     return CSRGraph(n=n, row_ptr=row_ptr.cpu().numpy(), col=col.cpu().numpy(), w=None, name=name)
+
+
+@dataclasses.dataclass
+class PackedBatch:
+    """Many graphs packed into one CSR on a device: vertex ranges vtx_offsets[g]..[g+1],
+    global column IDs, unit weights. Tensors are torch (int64 offsets/row_ptr, int32 col)."""
+    vtx_offsets: object
+    row_ptr: object
+    col: object
+    n: np.ndarray   # vertices per graph (host)
+    m: np.ndarray   # undirected edges per graph (host)
+    name: str = ""
+
+    @property
+    def G(self) -> int:
+        return int(self.n.size)
+
+    def graph(self, g: int):
+        """Graph g as (n, row_ptr, col) device tensors with local IDs (for single-graph runs)."""
+        import torch
+        vb = int(self.vtx_offsets[g]); ve = int(self.vtx_offsets[g + 1])
+        rp = self.row_ptr[vb: ve + 1]
+        e0 = int(rp[0])
+        return ve - vb, (rp - e0).contiguous(), (self.col[e0: int(rp[-1])] - vb).to(torch.int32).contiguous()
+
+
+def _device_csr_from_keys(lo, hi, n_total: int, vtx_offsets_old, device):
+    """Deduplicated undirected pairs (global IDs) -> packed CSR with isolated vertices dropped
+    and IDs compacted in ascending order; vertex offsets move with the compaction."""
+    import torch
+    key = torch.unique((lo << 32) | hi)
+    lo = key >> 32
+    hi = key & 0xFFFFFFFF
+    del key
+    ids = torch.unique(torch.cat([lo, hi]))
+    lo = torch.searchsorted(ids, lo)
+    hi = torch.searchsorted(ids, hi)
+    offs = torch.searchsorted(ids, vtx_offsets_old)
+    n = int(ids.numel())
+    del ids
+    k2 = torch.sort(torch.cat([(lo << 32) | hi, (hi << 32) | lo])).values
+    del lo, hi
+    src = k2 >> 32
+    col = (k2 & 0xFFFFFFFF).to(torch.int32)
+    del k2
+    counts = torch.bincount(src, minlength=n)
+    del src
+    row_ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    row_ptr[1:] = torch.cumsum(counts, 0)
+    return offs, row_ptr, col
+
+
+def chung_lu_batch_device(G: int = 4096, n_min: int = 200, n_max: int = 200_000,
+                          exponent: float = 2.1, mean_degree: float = 8.0, seed: int = 1,
+                          device="cuda") -> PackedBatch:
+    """The batched workload, generated on a CUDA device with torch: G independent Chung-Lu
+    graphs (the ``chung_lu_mean`` weight sequence w_i ~ (i+1)^(-1/(exponent-1)), mean degree
+    fixed, weights capped at sqrt(sum)), vertex counts log-uniform in [n_min, n_max], each
+    graph's IDs randomly permuted, canonicalised per graph and packed. Vertex counts come from
+    numpy's PCG64 with ``seed``; the endpoints from torch's device generator with ``seed``."""
+    import torch
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(n_min), math.log(n_max), G)).astype(np.int64)
+    ms = np.rint(mean_degree * ns / 2.0).astype(np.int64)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    ns_t = torch.from_numpy(ns).to(device)
+    voff = torch.zeros(G + 1, dtype=torch.int64, device=device)
+    voff[1:] = torch.cumsum(ns_t, 0)
+    N = int(ns.sum())
+    gid = torch.repeat_interleave(torch.arange(G, device=device), ns_t)
+    local = torch.arange(N, device=device, dtype=torch.int64) - voff[gid]
+    wts = (local.to(torch.float64) + 1.0) ** (-1.0 / (exponent - 1.0))
+    del local
+    wsum = torch.zeros(G, dtype=torch.float64, device=device).index_add_(0, gid, wts)
+    wts *= (mean_degree * ns_t.to(torch.float64) / wsum)[gid]
+    wts = torch.minimum(wts, torch.sqrt(mean_degree * ns_t.to(torch.float64))[gid])
+    # per-graph CDF shifted by the graph index: segment g covers (g, g + 1]
+    c = torch.cumsum(wts, 0)
+    del wts
+    start = torch.zeros(G, dtype=torch.float64, device=device)
+    start[1:] = c[voff[1:-1] - 1]
+    total = c[voff[1:] - 1] - start
+    cdf = (c - start[gid]) / total[gid] + gid.to(torch.float64)
+    del c
+    ms_t = torch.from_numpy(ms).to(device)
+    eg = torch.repeat_interleave(torch.arange(G, device=device), ms_t)
+    last = voff[1:] - 1
+
+    def endpoints():
+        r = torch.rand(eg.numel(), generator=gen, device=device, dtype=torch.float64) + eg.to(torch.float64)
+        return torch.minimum(torch.searchsorted(cdf, r, right=True), last[eg])
+
+    u = endpoints()
+    v = endpoints()
+    del cdf
+    # random relabelling inside each graph so hubs are not all at low IDs
+    keys = torch.rand(N, generator=gen, device=device, dtype=torch.float64) + gid.to(torch.float64)
+    order = torch.argsort(keys)
+    del keys
+    newid = torch.empty_like(order)
+    newid[order] = torch.arange(N, device=device, dtype=torch.int64)
+    del order
+    u = newid[u]
+    v = newid[v]
+    del newid, eg, gid
+    keep = u != v
+    u, v = u[keep], v[keep]
+    lo = torch.minimum(u, v)
+    hi = torch.maximum(u, v)
+    del u, v, keep
+    offs, row_ptr, col = _device_csr_from_keys(lo, hi, N, voff, device)
+    offs_h = offs.cpu().numpy()
+    rp_h = row_ptr[offs].cpu().numpy()
+    n_out = np.diff(offs_h)
+    m_out = np.diff(rp_h) // 2
+    return PackedBatch(offs, row_ptr, col, n_out, m_out,
+                       name=f"chung_lu_batch_G{G}_n{n_min}-{n_max}_g{exponent}_k{mean_degree}_s{seed}")
+
+
+def rmat_device(n_target: int, edge_factor: int = 8, a: float = 0.57, b: float = 0.19,
+                c: float = 0.19, seed: int = 1, device="cuda") -> CSRGraph:
+    """R-MAT graph with about n_target vertices, generated on a CUDA device: edge_factor *
+    n_target edges drawn at scale ceil(log2 n_target), IDs scaled down onto [0, n_target)
+    (u * n_target >> scale keeps the skew), then canonicalised (host CSR returned)."""
+    import torch
+    scale = max(1, int(math.ceil(math.log2(max(2, n_target)))))
+    n_edges = edge_factor * n_target
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    u = torch.zeros(n_edges, dtype=torch.int64, device=device)
+    v = torch.zeros(n_edges, dtype=torch.int64, device=device)
+    ab, abc = a + b, a + b + c
+    for _ in range(scale):
+        r = torch.rand(n_edges, generator=gen, device=device, dtype=torch.float32)
+        ubit = r >= ab
+        vbit = ((r >= a) & (r < ab)) | (r >= abc)
+        u = (u << 1) | ubit
+        v = (v << 1) | vbit
+    u = (u * n_target) >> scale
+    v = (v * n_target) >> scale
+    return to_device_canonical(u, v, device=device, name=f"rmat_n{n_target}_ef{edge_factor}_s{seed}")
