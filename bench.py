@@ -239,7 +239,9 @@ def run_batched(args, local):
     torch.cuda.set_device(local)
     b = graphs.chung_lu_batch_device(G=args.graphs, seed=SEED, device=dev)
     mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
-    eng = lv.Engine(local, mode=mode)
+    # the batch runs as one captured level loop (CUDA graph with device-side loop control)
+    eng = lv.Engine(local, mode=mode, use_graphs=True)
+    plain = lv.Engine(local, mode=mode)
     N = int(b.n.sum())
     out_d = torch.empty(N, dtype=torch.int32, device=dev)
     for _ in range(max(1, args.warmup)):
@@ -257,13 +259,13 @@ def run_batched(args, local):
     singles = [b.graph(g) for g in range(b.G)]
     outs = [torch.empty(n, dtype=torch.int32, device=dev) for n, _, _ in singles]
     for g in range(min(8, b.G)):
-        eng.run_csr(singles[g][0], singles[g][1], singles[g][2], None, out=outs[g])
+        plain.run_csr(singles[g][0], singles[g][1], singles[g][2], None, out=outs[g])
     torch.cuda.synchronize()
     q_loop = np.empty(b.G)
     t0 = time.perf_counter()
     loop_launches = 0
     for g, (n, rp, col) in enumerate(singles):
-        _, q_loop[g], s1 = eng.run_csr(n, rp, col, None, out=outs[g])
+        _, q_loop[g], s1 = plain.run_csr(n, rp, col, None, out=outs[g])
         loop_launches += s1.kernel_launches
     torch.cuda.synchronize()
     loop_ms = (time.perf_counter() - t0) * 1e3
@@ -287,8 +289,10 @@ def run_batched(args, local):
         "levels": st.levels, "passes": st.iterations, "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    line["graph_launches"] = int(st.graph_launches)
     print(json.dumps(line), flush=True)
     eng.close()
+    plain.close()
     return 0
 
 

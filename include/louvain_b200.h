@@ -75,8 +75,9 @@ typedef struct {
   int32_t weight_mode;      /* lv_weight_mode; default LV_WEIGHTS_AUTO */
   int32_t validate;         /* 1 = check row_ptr monotone / col in range / no empty row on
                                the device before running (default 1) */
-  int32_t use_graphs;       /* 1 = run each level's iteration loop as a captured CUDA graph
-                               with device-side loop control (default 1) */
+  int32_t use_graphs;       /* 1 = run the level loop (passes, aggregation, next level) as one
+                               captured CUDA graph with device-side loop control;
+                               0 = host-driven, one stream launch sequence per pass (default) */
   int32_t reserved_i[7];
   /* degree-bin tiling; 0 = use the autotuned or built-in table */
   int32_t bin_max_degree[8];
@@ -107,7 +108,9 @@ typedef struct {
   int64_t kernel_launches;      /* engine kernels launched by the call */
   int64_t active_entries;       /* sum over passes of the active vertices' entries */
   int64_t active_vertices;      /* sum over passes of the active vertices */
-  int64_t reserved[3];
+  int64_t graph_launches;       /* launches of the captured level loop (0: host-driven run;
+                                   more than 1 when the run stopped to grow its hash arena) */
+  int64_t reserved[2];
 } lv_stats;
 
 typedef struct lv_context lv_context;

@@ -70,7 +70,7 @@ class Stats(ctypes.Structure):
         ("bytes_optimization", ctypes.c_double), ("ms_optimization_kernels", ctypes.c_float),
         ("reserved1", ctypes.c_int32), ("kernel_launches", ctypes.c_int64),
         ("active_entries", ctypes.c_int64), ("active_vertices", ctypes.c_int64),
-        ("reserved", ctypes.c_int64 * 3),
+        ("graph_launches", ctypes.c_int64), ("reserved", ctypes.c_int64 * 2),
     ]
 
     def as_dict(self) -> dict:
@@ -176,7 +176,7 @@ def _is_device(a) -> bool:
 def config(mode: int = MODE.SORT, threshold: float = 1e-3, fast_first: bool = True,
            chunk_edges: int = 50_000_000, max_iterations: int = 1_000_000_000,
            max_levels: int = 0, weight_mode: int = WEIGHTS_AUTO,
-           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = True) -> Config:
+           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = False) -> Config:
     c = Config()
     load_library().lv_config_default(ctypes.byref(c))
     c.mode = int(mode)

@@ -38,7 +38,13 @@ enum : uint32_t {
   kErrInput = 1u << 3,        // input validation: col out of range / empty row / bad weight
   kErrChunks = 1u << 4,       // more edge chunks than the emulation supports
   kErrRange = 1u << 5,        // integer mode: total weight >= 2^32
+  kErrLoop = 1u << 6,         // captured run: pass or level count beyond its guard
 };
+
+// Guards of the captured run's device-side loops (far beyond any real run: Louvain's passes
+// and levels each raise the modularity by more than the threshold, so both counts are small).
+constexpr uint32_t kGuardPasses = 1u << 24;
+constexpr uint32_t kGuardLevels = 1u << 16;
 
 constexpr int kMaxChunks = 1024;
 constexpr int kNumBins = 8;
@@ -115,8 +121,35 @@ struct Ctrl {
   unsigned long long act_vertices_total;  // summed over the run's passes
   unsigned long long act_entries_total;
   double threshold;
+  // device-driven runs (a captured graph with conditional nodes): why the graph stopped early
+  // (0 none, kAbortAggArena / kAbortOptArena), the arena slots that were needed, per-run counts
+  // of the captured segments that ran, and device-clock phase times in ns (%globaltimer)
+  uint32_t abort;
+  uint32_t pad_abort;
+  unsigned long long arena_need;  // slots wanted by the global-table bin at this level start
+  unsigned long long abort_need;
+  uint32_t seg_levels, seg_passes, seg_aggs, seg_contract, seg_contract_ok, seg_final;
+  unsigned long long t_pass0, t_agg0, t_opt_ns, t_optk_ns, t_agg_ns;
   TraceRec trace[kTraceCap];
 };
+
+constexpr uint32_t kAbortAggArena = 1;  // aggregation: contraction tables beyond the arena
+constexpr uint32_t kAbortOptArena = 2;  // level start: optimisation tables beyond the arena
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Conditional-node handles of a captured run (on = 0: plain stream launches, no handles).
+struct GraphCtl {
+  unsigned long long level, pass, contract, ok;  // cudaGraphConditionalHandle values
+  int on;
+};
+__device__ __forceinline__ void set_cond(const GraphCtl& gc, unsigned long long h, bool v) {
+  if (gc.on) cudaGraphSetConditional((cudaGraphConditionalHandle)h, v ? 1u : 0u);
+}
 
 // ---- reference arithmetic -----------------------------------------------------------------
 // operatorsDelta.h:29-45 (DeltaModularitySort / DeltaModularityHash): the float difference

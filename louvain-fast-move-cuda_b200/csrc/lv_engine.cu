@@ -18,6 +18,8 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/louvain_b200.h"
@@ -133,6 +135,21 @@ static void ensure_dyn_smem(int device, const void* fn, size_t bytes) {
   cur = bytes;
 }
 
+// Resident blocks per SM of a kernel at a block size and dynamic shared memory, cached per
+// process (the occupancy calculator is not free and every run asks the same questions).
+static int occupancy(int device, const void* fn, int block, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_tuple(device, fn, block, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int occ = 0;
+  LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem));
+  cache.emplace(key, occ);
+  return occ;
+}
+
 struct HostCtrlSnap {
   uint32_t it, n, E, n0, G, n_iterating, err, fast, rule_sort;
 };
@@ -167,18 +184,19 @@ class Run {
   std::vector<Block> arena_blocks;
 
   // stream == nullptr: the context's stream and readback buffer (calls serialised by the
-  // context lock); otherwise a private stream, as the serving loop runs several at once.
-  explicit Run(lv_context* c, cudaStream_t stream = nullptr) : ctx(c), cfg(c->cfg) {
+  // context lock); otherwise a private stream, as the serving loop runs several at once, with
+  // the caller's 64-byte pinned readback buffer (or one of the run's own if none is given).
+  explicit Run(lv_context* c, cudaStream_t stream = nullptr, uint32_t* pinned_buf = nullptr)
+      : ctx(c), cfg(c->cfg) {
     for (auto& e : ev) e = nullptr;
     st = stream ? stream : c->stream;
-    if (stream) {
-      own_pinned = true;
-    } else {
-      pinned = c->pinned;
-    }
+    pinned = stream ? pinned_buf : c->pinned;
   }
   ~Run() {
     cudaStreamSynchronize(st);
+    release_graph();
+    for (cudaStream_t x : cs)
+      if (x) cudaStreamDestroy(x);
     for (const Block& b : owned) ctx->give(b.p, b.bytes);
     for (const Block& b : arena_blocks) ctx->give(b.p, b.bytes);
     if (own_pinned && pinned) cudaFreeHost(pinned);
@@ -211,6 +229,7 @@ class Run {
     LV_CUDA(cudaGetLastError());
     if (e & kErrInput) throw Fail{LV_ERR_INPUT, "input graph: a row is empty, a column index is outside its graph, or a weight is invalid for the weight mode"};
     if (e & kErrRange) throw Fail{LV_ERR_RANGE, "integer weights: total weight 2m must be below 2^32 (the reference sums in u32)"};
+    if (e & kErrLoop) throw Fail{LV_ERR_DEVICE_CHECK, "captured run: pass or level guard tripped"};
     if (e) throw Fail{LV_ERR_DEVICE_CHECK, "device check failed (flags " + std::to_string(e) + ")"};
   }
 
@@ -239,9 +258,7 @@ class Run {
     const size_t smem = (size_t)(256 / T) * team_cap[b] * (4 + acc_size());
     ensure_dyn_smem(ctx->device, opt_fn, smem);
     ensure_dyn_smem(ctx->device, con_fn, smem);
-    int occ = 0;
-    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, opt_fn, 256, smem));
-    grid_team[b] = ctx->sms * std::max(1, occ);
+    grid_team[b] = ctx->sms * std::max(1, occupancy(ctx->device, opt_fn, 256, smem));
   }
 
   template <bool WI>
@@ -255,9 +272,7 @@ class Run {
     const size_t bsmem = (size_t)block_cap * (4 + acc_size());
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI, false>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, bsmem);
-    int occ = 0;
-    LV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_opt_block<WI, false>, 512, bsmem));
-    grid_block[0] = ctx->sms * std::max(1, occ);
+    grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI, false>, 512, bsmem));
   }
 
   // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
@@ -265,72 +280,144 @@ class Run {
             const float* w, int in_mem) {
     if (n_ <= 0 || !row_ptr || !col) throw Fail{LV_ERR_ARGUMENT, "n must be positive; row_ptr and col are required"};
     if (n_ >= 0xFFFFFFFFll) throw Fail{LV_ERR_RANGE, "more than 2^32-2 vertices"};
-    G = G_;
-    n0 = n = (uint32_t)n_;
-    const cudaMemcpyKind kin = in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     int64_t E64 = 0;
-    LV_CUDA(cudaMemcpyAsync(&E64, row_ptr + n_, sizeof(int64_t),
-                            in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, st));
-    sync();
+    if (in_mem == LV_MEM_DEVICE) {
+      LV_CUDA(cudaMemcpyAsync(&E64, row_ptr + n_, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      sync();
+    } else {
+      E64 = row_ptr[n_];
+    }
+    std::vector<int64_t> ho(G_ + 1);
+    if (G_ > 1) {
+      if (in_mem == LV_MEM_DEVICE) {
+        LV_CUDA(cudaMemcpyAsync(ho.data(), offs, (G_ + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        sync();
+      } else {
+        std::memcpy(ho.data(), offs, (G_ + 1) * sizeof(int64_t));
+      }
+      if (ho[0] != 0 || ho[G_] != n_) throw Fail{LV_ERR_ARGUMENT, "vtx_offsets must start at 0 and end at n"};
+      for (uint32_t g = 0; g < G_; ++g)
+        if (ho[g + 1] <= ho[g]) throw Fail{LV_ERR_INPUT, "every graph of a batch needs at least one vertex"};
+    } else {
+      ho[0] = 0;
+      ho[1] = n_;
+    }
+    allocate(G_, n_, E64);
+    const cudaMemcpyKind kin = in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (w) LV_CUDA(cudaMemcpyAsync(D.w, w, (size_t)E * 4, kin, st));
+    choose_weight_mode(w != nullptr);
+    LV_CUDA(cudaMemcpyAsync(D.col, col, (size_t)E * 4, kin, st));
+    LV_CUDA(cudaMemcpyAsync(row64(), row_ptr, (size_t)(n + 1) * 8, kin, st));
+    long long* doffs = nullptr;
+    if (G > 1) {
+      doffs = dalloc<long long>(ctx, owned, (size_t)G + 1);
+      LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
+    }
+    prepare(ho, doffs, w != nullptr);
+  }
+
+  // A batch assembled from separate host graphs (local numbering each): every piece is
+  // uploaded into its place in the packed buffers and rebased on the device.
+  struct Piece {
+    int64_t n, E;
+    const int64_t* row;
+    const int32_t* col;
+    const float* w;
+  };
+  void init_pieces(const std::vector<Piece>& ps) {
+    if (ps.empty()) throw Fail{LV_ERR_ARGUMENT, "empty batch"};
+    std::vector<int64_t> ho(ps.size() + 1, 0), eo(ps.size() + 1, 0);
+    for (size_t g = 0; g < ps.size(); ++g) {
+      if (ps[g].n <= 0 || ps[g].E <= 0 || !ps[g].row || !ps[g].col) throw Fail{LV_ERR_ARGUMENT, "invalid batch piece"};
+      if ((ps[g].w != nullptr) != (ps[0].w != nullptr)) throw Fail{LV_ERR_ARGUMENT, "a batch is all weighted or all unweighted"};
+      ho[g + 1] = ho[g] + ps[g].n;
+      eo[g + 1] = eo[g] + ps[g].E;
+    }
+    if (ho.back() >= 0xFFFFFFFFll) throw Fail{LV_ERR_RANGE, "more than 2^32-2 vertices"};
+    allocate((uint32_t)ps.size(), ho.back(), eo.back());
+    const bool weighted = ps[0].w != nullptr;
+    long long* r64 = row64();
+    for (size_t g = 0; g < ps.size(); ++g) {
+      if (weighted)
+        LV_CUDA(cudaMemcpyAsync(reinterpret_cast<float*>(D.w) + eo[g], ps[g].w, (size_t)ps[g].E * 4,
+                                cudaMemcpyHostToDevice, st));
+      LV_CUDA(cudaMemcpyAsync(D.col + eo[g], ps[g].col, (size_t)ps[g].E * 4, cudaMemcpyHostToDevice, st));
+      LV_CUDA(cudaMemcpyAsync(r64 + ho[g], ps[g].row, (size_t)ps[g].n * 8, cudaMemcpyHostToDevice, st));
+    }
+    long long* doffs = dalloc<long long>(ctx, owned, 2 * ((size_t)G + 1));
+    LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
+    LV_CUDA(cudaMemcpyAsync(doffs + G + 1, eo.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
+    k_rebase_pieces<<<ctx->sms * 4, 256, 0, st>>>(r64, D.col, doffs, doffs + G + 1, G, n, E);
+    ++launches;
+    choose_weight_mode(weighted);
+    prepare(ho, doffs, weighted);
+  }
+
+ private:
+  long long* row64() { return reinterpret_cast<long long*>(D.cd); }  // (n+1) x 8 B, free until aggregation
+
+  void allocate(uint32_t G_, int64_t n_, int64_t E64) {
     if (E64 <= 0) throw Fail{LV_ERR_INPUT, "graph has no edges"};
     // hash tables are sized next_pow2(2 x row length) in u32 arithmetic
     if (E64 > (1ll << 30)) throw Fail{LV_ERR_RANGE, "more than 2^30 edge entries"};
+    G = G_;
+    n0 = n = (uint32_t)n_;
     E = (uint32_t)E64;
     m_edges = E64 / 2;
-    if (own_pinned) LV_CUDA(cudaMallocHost(&pinned, 64));
+    if (!pinned) {
+      LV_CUDA(cudaMallocHost(&pinned, 64));
+      own_pinned = true;
+    }
     for (auto& e : ev) LV_CUDA(cudaEventCreate(&e));
-
     // device arrays (level-0 sizes, reused by every level)
-    D.row = dalloc<uint32_t>(ctx, owned,n + 1);
-    D.rowB = dalloc<uint32_t>(ctx, owned,n + 1);
-    D.col = dalloc<uint32_t>(ctx, owned,E);
-    D.colB = dalloc<uint32_t>(ctx, owned,E);
-    D.w = dalloc<uint32_t>(ctx, owned,E);
-    D.wB = dalloc<uint32_t>(ctx, owned,E);
-    D.k = dalloc<double>(ctx, owned,n);
-    D.kB = dalloc<double>(ctx, owned,n);
-    D.comm = dalloc<uint32_t>(ctx, owned,n);
-    D.a = dalloc<double>(ctx, owned,n);
-    D.new_comm = dalloc<uint32_t>(ctx, owned,n);
-    D.moved_it = dalloc<uint32_t>(ctx, owned,n);
-    D.active_it = dalloc<uint32_t>(ctx, owned,n);
-    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned,n);
-    D.hub_off = dalloc<uint32_t>(ctx, owned,n);
+    D.row = dalloc<uint32_t>(ctx, owned, n + 1);
+    D.rowB = dalloc<uint32_t>(ctx, owned, n + 1);
+    D.col = dalloc<uint32_t>(ctx, owned, E);
+    D.colB = dalloc<uint32_t>(ctx, owned, E);
+    D.w = dalloc<uint32_t>(ctx, owned, E);
+    D.wB = dalloc<uint32_t>(ctx, owned, E);
+    D.k = dalloc<double>(ctx, owned, n);
+    D.kB = dalloc<double>(ctx, owned, n);
+    D.comm = dalloc<uint32_t>(ctx, owned, n);
+    D.a = dalloc<double>(ctx, owned, n);
+    D.new_comm = dalloc<uint32_t>(ctx, owned, n);
+    D.moved_it = dalloc<uint32_t>(ctx, owned, n);
+    D.active_it = dalloc<uint32_t>(ctx, owned, n);
+    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n);
+    D.hub_off = dalloc<uint32_t>(ctx, owned, n);
     D.hubtab = dalloc<uint32_t>(ctx, owned, n);
     D.hubself = dalloc<unsigned long long>(ctx, owned, n);
     D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
     D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
-    D.movers = dalloc<uint32_t>(ctx, owned,n);
-    D.gs = dalloc<GraphState>(ctx, owned,G);
-    D.ctrl = dalloc<Ctrl>(ctx, owned,1);
-    D.partials = dalloc<double>(ctx, owned,kMaxPartials);
-    D.map = dalloc<unsigned long long>(ctx, owned,n);
-    D.cd = dalloc<unsigned long long>(ctx, owned,(size_t)n + 1);
-    D.rank = dalloc<uint32_t>(ctx, owned,n);
-    D.members = dalloc<uint32_t>(ctx, owned,n);
-    D.newdeg = dalloc<uint32_t>(ctx, owned,(size_t)n + 1);
-    D.best = dalloc<uint32_t>(ctx, owned,n0);
-    D.out = dalloc<int32_t>(ctx, owned,n0);
+    D.movers = dalloc<uint32_t>(ctx, owned, n);
+    D.gs = dalloc<GraphState>(ctx, owned, G);
+    D.ctrl = dalloc<Ctrl>(ctx, owned, 1);
+    D.partials = dalloc<double>(ctx, owned, kMaxPartials);
+    D.map = dalloc<unsigned long long>(ctx, owned, n);
+    D.cd = dalloc<unsigned long long>(ctx, owned, (size_t)n + 1);
+    D.rank = dalloc<uint32_t>(ctx, owned, n);
+    D.members = dalloc<uint32_t>(ctx, owned, n);
+    D.newdeg = dalloc<uint32_t>(ctx, owned, (size_t)n + 1);
+    D.best = dalloc<uint32_t>(ctx, owned, n0);
+    D.out = dalloc<int32_t>(ctx, owned, n0);
     if (G > 1) {
-      D.gid = dalloc<uint32_t>(ctx, owned,n);
-      D.gidB = dalloc<uint32_t>(ctx, owned,n);
-      D.gid0 = dalloc<uint32_t>(ctx, owned,n0);
+      D.gid = dalloc<uint32_t>(ctx, owned, n);
+      D.gidB = dalloc<uint32_t>(ctx, owned, n);
+      D.gid0 = dalloc<uint32_t>(ctx, owned, n0);
     }
-    scan_tmp = dalloc<unsigned long long>(ctx, owned,(size_t)(n + 1) / kScanTile + 2);
-    scan_tot = dalloc<unsigned long long>(ctx, owned,1);
+    scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2);
+    scan_tot = dalloc<unsigned long long>(ctx, owned, 1);
+  }
 
-    // weight mode
-    float* w_dev_tmp = nullptr;
-    if (w) {
-      LV_CUDA(cudaMemcpyAsync(D.w, w, (size_t)E * 4, kin, st));
-      w_dev_tmp = reinterpret_cast<float*>(D.w);
-    }
+  // Integer or float semantics (the weights, if any, are already in D.w), then the bin tables.
+  void choose_weight_mode(bool weighted) {
     int wm = cfg.weight_mode;
-    if (!w) wm = LV_WEIGHTS_INTEGER;
+    if (!weighted) wm = LV_WEIGHTS_INTEGER;
     if (wm == LV_WEIGHTS_AUTO) {
       uint32_t* flag = reinterpret_cast<uint32_t*>(D.partials);
       LV_CUDA(cudaMemsetAsync(flag, 0, 4, st));
-      k_weights_integral<<<ctx->sms * 4, 256, 0, st>>>(w_dev_tmp, E, flag);
+      k_weights_integral<<<ctx->sms * 4, 256, 0, st>>>(reinterpret_cast<const float*>(D.w), E, flag);
+      ++launches;
       LV_CUDA(cudaMemcpyAsync(pinned, flag, 4, cudaMemcpyDeviceToHost, st));
       sync();
       wm = pinned[0] ? LV_WEIGHTS_FLOAT : LV_WEIGHTS_INTEGER;
@@ -340,12 +427,10 @@ class Run {
     if (wint) configure_kernels<true>(); else configure_kernels<false>();
     grid_n = ctx->sms * 8;
     grid_sq = std::min(kMaxPartials, ctx->sms * 4);
+  }
 
-    LV_CUDA(cudaMemcpyAsync(D.col, col, (size_t)E * 4, kin, st));
-    long long* row64 = reinterpret_cast<long long*>(D.cd);  // (n+1) x 8 bytes, free until aggregation
-    LV_CUDA(cudaMemcpyAsync(row64, row_ptr, (size_t)(n + 1) * 8, kin, st));
-
-    // control block + graph states
+  // Control block, graph states, graph ids, degrees and totals, then the first level.
+  void prepare(const std::vector<int64_t>& ho, const long long* doffs, bool weighted) {
     LV_CUDA(cudaMemsetAsync(D.ctrl, 0, sizeof(Ctrl), st));
     LV_CUDA(cudaMemsetAsync(D.gs, 0, sizeof(GraphState) * G, st));
     Ctrl hc{};
@@ -356,17 +441,6 @@ class Run {
     hc.threshold = cfg.threshold;
     LV_CUDA(cudaMemcpyAsync(D.ctrl, &hc, offsetof(Ctrl, trace), cudaMemcpyHostToDevice, st));
     std::vector<GraphState> hs(G);
-    std::vector<int64_t> ho(G + 1);
-    if (G > 1) {
-      LV_CUDA(cudaMemcpyAsync(ho.data(), offs, (G + 1) * sizeof(int64_t),
-                              in_mem == LV_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, st));
-      sync();
-      if (ho[0] != 0 || ho[G] != n_) throw Fail{LV_ERR_ARGUMENT, "vtx_offsets must start at 0 and end at n"};
-      for (uint32_t g = 0; g < G; ++g)
-        if (ho[g + 1] <= ho[g]) throw Fail{LV_ERR_INPUT, "every graph of a batch needs at least one vertex"};
-    } else {
-      ho[0] = 0; ho[1] = n_;
-    }
     for (uint32_t g = 0; g < G; ++g) {
       std::memset(&hs[g], 0, sizeof(GraphState));
       hs[g].vb = (uint32_t)ho[g];
@@ -375,23 +449,24 @@ class Run {
     }
     LV_CUDA(cudaMemcpyAsync(D.gs, hs.data(), sizeof(GraphState) * G, cudaMemcpyHostToDevice, st));
     if (G > 1) {
-      long long* doffs = dalloc<long long>(ctx, owned,(size_t)G + 1);
-      LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
       k_fill_gid<<<std::min<uint32_t>(G, 65535), 256, 0, st>>>(D.gid, doffs, G);
       LV_CUDA(cudaMemcpyAsync(D.gid0, D.gid, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+      ++launches;
     }
+    const float* wf = weighted ? reinterpret_cast<const float*>(D.w) : nullptr;
     iota_best();
-    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
-    else k_prep<false><<<grid_n, 256, 0, st>>>(D, row64, w_dev_tmp, n, E);
-    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(D, w_dev_tmp);
-    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(D, w_dev_tmp);
+    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(D, row64(), wf, n, E);
+    else k_prep<false><<<grid_n, 256, 0, st>>>(D, row64(), wf, n, E);
+    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(D, wf);
+    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(D, wf);
     if (wint) k_prep_total<true><<<1, 256, 0, st>>>(D);
     else k_prep_total<false><<<1, 256, 0, st>>>(D);
-    launches += 4 + (G > 1 ? 1 : 0) + (w && cfg.weight_mode == LV_WEIGHTS_AUTO ? 1 : 0);
+    launches += 4;
     check_device_errors();
     level_start();
   }
 
+ public:
   unsigned long long* scan_tmp = nullptr;
   unsigned long long* scan_tot = nullptr;
 
@@ -399,13 +474,14 @@ class Run {
 
   // ---- scans --------------------------------------------------------------------------------
   template <class T, bool INCL>
-  void scan(const T* in, T* out, uint32_t count) {
+  void scan(const T* in, T* out, uint32_t count, const uint32_t* dcount = nullptr, uint32_t add = 0) {
+    // count: the length (dcount == nullptr) or an upper bound of *dcount + add (the grid)
     if (count == 0) return;
     const uint32_t tiles = (count + kScanTile - 1) / kScanTile;
     T* tmp = reinterpret_cast<T*>(scan_tmp);
-    k_scan_tiles<T><<<tiles, kScanNT, 0, st>>>(in, tmp, count);
-    k_scan_sums<T><<<1, 1024, 0, st>>>(tmp, tiles);
-    k_scan_apply<T, INCL><<<tiles, kScanNT, 0, st>>>(in, out, tmp, count, nullptr);
+    k_scan_tiles<T><<<tiles, kScanNT, 0, st>>>(in, tmp, count, dcount, add);
+    k_scan_sums<T><<<1, 1024, 0, st>>>(tmp, tiles, dcount, add);
+    k_scan_apply<T, INCL><<<tiles, kScanNT, 0, st>>>(in, out, tmp, count, dcount, add);
     launches += 3;
   }
 
@@ -415,8 +491,8 @@ class Run {
     else k_commit_sq<false><<<grid_sq, 256, 0, st>>>(D, single() ? 1 : 0);
   }
   void finalize(int level_start_flag) {
-    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first);
-    else k_finalize<false><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first);
+    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
+    else k_finalize<false><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
   }
 
   void ensure_arena(uint64_t need_slots) {
@@ -438,22 +514,21 @@ class Run {
     write_ctrl_u32(offsetof(Ctrl, arena_slots), (uint32_t)slots);
   }
 
-  void level_start() {
-    if (single() && cfg.chunk_edges > 0)
+  // Community::update at a new level, then the arena the level's global tables need.
+  void level_start_kernels() {
+    if (single() && cfg.chunk_edges > 0) {
       k_chunk_bounds<<<1, 1, 0, st>>>(D, (unsigned long long)cfg.chunk_edges);
+      ++launches;
+    }
     k_level_init<<<grid_n, 256, 0, st>>>(D);
     commit_sq();
     finalize(1);
-    // global tables for the highest-degree vertices of this level
-    unsigned long long* need = scan_tot;
-    LV_CUDA(cudaMemsetAsync(need, 0, 8, st));
-    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], bins.block_cap, need);
-    launches += 4 + ((single() && cfg.chunk_edges > 0) ? 1 : 0);
-    LV_CUDA(cudaMemcpyAsync(pinned, need, 8, cudaMemcpyDeviceToHost, st));
-    sync();
-    uint64_t nd;
-    std::memcpy(&nd, pinned, 8);
-    ensure_arena(nd);
+    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], bins.block_cap);
+    launches += 4;
+  }
+  void level_start() {
+    level_start_kernels();
+    ensure_arena(read_ctrl<unsigned long long>(offsetof(Ctrl, arena_need)));
     check_device_errors();
   }
 
@@ -461,7 +536,7 @@ class Run {
   template <bool WI>
   void launch_pass() {
     const size_t slot = 4 + (WI ? 4 : 8);
-    LV_CUDA(cudaEventRecord(ev[4], st));
+    if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
     k_chunk_flags<<<grid_n, 256, 0, st>>>(D);
     k_bin_vertices<<<grid_n, 256, 0, st>>>(D, bins);
     k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
@@ -476,7 +551,7 @@ class Run {
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
     k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
     k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(D);
-    LV_CUDA(cudaEventRecord(ev[5], st));
+    if (!gc.on) LV_CUDA(cudaEventRecord(ev[5], st));
     k_apply<WI><<<grid_n, 256, 0, st>>>(D);
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(D);
     commit_sq();
@@ -505,25 +580,66 @@ class Run {
   }
 
   // ---- aggregation --------------------------------------------------------------------------------
+  // Split at the points where a host-driven run reads sizes back and a captured run branches:
+  // renumbering (prefix), binning of the new communities (contract_a), the arena-backed
+  // contraction (contract_b), best-partition update and level switch (tail). Everything before
+  // the tail can run again from the start with the same result, so a captured run may stop at
+  // the arena check and let the host redo the aggregation with a larger arena.
+  template <bool WI>
+  void agg_prefix(int force) {
+    const uint32_t gb = std::max<uint32_t>(1, (G + 255) / 256);
+    k_agg_decide<<<gb, 256, 0, st>>>(D, force, (uint32_t)std::max(0, cfg.max_levels));
+    k_agg_clear_map<<<grid_n, 256, 0, st>>>(D);
+    k_agg_mark<<<grid_n, 256, 0, st>>>(D);
+    k_agg_flags<<<grid_n, 256, 0, st>>>(D);
+    scan<unsigned long long, true>(D.map, D.map, scan_bound(), &D.ctrl->n, 0);
+    k_agg_meta<<<gb, 256, 0, st>>>(D);
+    launches += 5;
+  }
+  template <bool WI>
+  void agg_contract_a() {
+    k_agg_clear_next<<<grid_n, 256, 0, st>>>(D);
+    k_agg_count<<<grid_n, 256, 0, st>>>(D);
+    scan<unsigned long long, false>(D.cd, D.cd, scan_bound() + 1, &D.ctrl->n_next, 1);
+    k_agg_scatter<<<grid_n, 256, 0, st>>>(D);
+    k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
+    launches += 4;
+  }
+  template <bool WI>
+  void agg_contract_b() {
+    const size_t slot = 4 + (WI ? 4 : 8);
+    // the largest new communities: many blocks insert into their global tables
+    k_arena_clear<<<ctx->sms * 8, 256, 0, st>>>(D);
+    k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(D, kNumBins - 1);
+    k_hub_insert<WI><<<grid_n, 256, 0, st>>>(D);
+    k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
+    k_hub_emit<WI><<<ctx->sms * 8, 512, 0, st>>>(D);
+    k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
+    k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
+    k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
+    k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
+    k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
+    k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
+    k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
+    scan<uint32_t, false>(D.newdeg, D.rowB, scan_bound() + 1, &D.ctrl->n_next, 1);
+    k_agg_compact<WI><<<grid_n, 256, 0, st>>>(D);
+    launches += 13;
+  }
+  void agg_tail() {
+    k_agg_best<<<grid_n, 256, 0, st>>>(D);
+    k_agg_finish<<<grid_n, 256, 0, st>>>(D);
+    launches += 2;
+  }
+  // Scan grids: exact level sizes when the host drives, level-0 sizes in a captured run.
+  uint32_t scan_bound() const { return gc.on ? n0 : n; }
+
   // Returns true if any graph continues to a new level.
   template <bool WI>
   bool aggregate_impl(int force) {
-    const size_t slot = 4 + (WI ? 4 : 8);
-    k_agg_decide<<<std::max<uint32_t>(1, (G + 255) / 256), 256, 0, st>>>(D, force, (uint32_t)std::max(0, cfg.max_levels));
-    LV_CUDA(cudaMemsetAsync(D.map, 0, (size_t)n * 8, st));
-    k_agg_mark<<<grid_n, 256, 0, st>>>(D);
-    k_agg_flags<<<grid_n, 256, 0, st>>>(D);
-    scan<unsigned long long, true>(D.map, D.map, n);
-    k_agg_meta<<<std::max<uint32_t>(1, (G + 255) / 256), 256, 0, st>>>(D);
-    k_agg_best<<<grid_n, 256, 0, st>>>(D);
+    agg_prefix<WI>(force);
     const uint32_t n2 = ctrl_u32(offsetof(Ctrl, n_next));
     if (n2 > 0) {
-      LV_CUDA(cudaMemsetAsync(D.cd, 0, ((size_t)n2 + 1) * 8, st));
-      k_agg_count<<<grid_n, 256, 0, st>>>(D);
-      scan<unsigned long long, false>(D.cd, D.cd, n2 + 1);
-      k_agg_scatter<<<grid_n, 256, 0, st>>>(D);
-      LV_CUDA(cudaMemsetAsync(D.hubtab, 0xFF, (size_t)n2 * 4, st));
-      k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
+      agg_contract_a<WI>();
       const uint32_t need = ctrl_u32(offsetof(Ctrl, hub_cursor));
       if (debug) {
         uint32_t bc[kNumBins];
@@ -533,30 +649,9 @@ class Run {
         std::fprintf(stderr, " hub_slots=%u\n", need);
       }
       ensure_arena(need);
-      if (need > 0) {
-        // the largest new communities: many blocks insert into their global tables
-        LV_CUDA(cudaMemsetAsync(D.arena_keys, 0xFF, (size_t)need * 4, st));
-        LV_CUDA(cudaMemsetAsync(D.arena_vals, 0, (size_t)need * 8, st));
-        k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(D, kNumBins - 1);
-        k_hub_insert<WI><<<grid_n, 256, 0, st>>>(D);
-        k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
-        k_hub_emit<WI><<<std::min<uint32_t>(need / kHubChunk, (uint32_t)ctx->sms * 8), 512, 0, st>>>(D, need / kHubChunk);
-        launches += 4;
-      }
-      k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
-      k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
-      k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
-      k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
-      k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
-      k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
-      k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
-      LV_CUDA(cudaMemsetAsync(D.newdeg + n2, 0, 4, st));
-      scan<uint32_t, false>(D.newdeg, D.rowB, n2 + 1);
-      k_agg_compact<WI><<<grid_n, 256, 0, st>>>(D);
-      launches += 11;
+      agg_contract_b<WI>();
     }
-    k_agg_finish<<<grid_n, 256, 0, st>>>(D);
-    launches += 6;
+    agg_tail();
     check_device_errors();
     n = ctrl_u32(offsetof(Ctrl, n));
     E = ctrl_u32(offsetof(Ctrl, E));
@@ -578,6 +673,205 @@ class Run {
     return cont;
   }
 
+  // ---- the captured run ------------------------------------------------------------------------------
+  // The whole level loop as one CUDA graph with device-side control:
+  //   while (level) {
+  //     k_gate_pass; while (pass) { <one pass, k_finalize sets `pass`> }
+  //     <aggregation prefix>; k_gate_contract
+  //     if (contract) { <binning>; k_gate_arena_agg
+  //                     if (ok) { <contraction>; <tail>; <level start>; k_gate_level } }
+  //     else          { <tail> }            (k_gate_contract cleared `level`)
+  //   }
+  // A launch runs every remaining level of every graph without a host round trip. It stops
+  // early only when a level needs a larger hash-table arena (Ctrl::abort says which); the host
+  // then grows the arena and continues, re-capturing because the arena pointers changed.
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  void* graph_arena = nullptr;  // arena the graph was captured with
+  GraphCtl gc{};
+  cudaStream_t cs[3] = {nullptr, nullptr, nullptr};
+  int64_t k_pass = 0, k_level = 0, k_contract = 0, k_ok = 0, k_final = 0;  // kernels per segment
+
+  void release_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+  }
+
+  // Adds a conditional node after the work captured so far on `s` and returns its body graphs.
+  cudaGraph_t* add_cond(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                        unsigned size) {
+    cudaStreamCaptureStatus status;
+    unsigned long long id = 0;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    LV_CUDA(cudaStreamGetCaptureInfo(s, &status, &id, &g, &deps, &nd));
+    if (status != cudaStreamCaptureStatusActive) throw Fail{LV_ERR_CUDA, "stream is not capturing"};
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = size;
+    cudaGraphNode_t node;
+    LV_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+    LV_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out;
+  }
+
+  // Captures `body` launched on stream s into graph g (st is switched to s meanwhile).
+  template <class F>
+  void capture_into(cudaGraph_t g, cudaStream_t s, F&& body) {
+    cudaStream_t saved = st;
+    st = s;
+    LV_CUDA(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t dummy = nullptr;
+      cudaStreamEndCapture(s, &dummy);
+      st = saved;
+      throw;
+    }
+    cudaGraph_t out = nullptr;
+    st = saved;
+    LV_CUDA(cudaStreamEndCapture(s, &out));
+  }
+
+  template <bool WI>
+  void build_graph() {
+    release_graph();
+    for (auto& x : cs)
+      if (!x) LV_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    LV_CUDA(cudaGraphCreate(&graph, 0));
+    // each handle belongs to the graph that holds its conditional node; only the level loop's
+    // handle has a launch default (1), the others are set by a gate kernel before their node
+    cudaGraphConditionalHandle hL, hP, hC, hO;
+    LV_CUDA(cudaGraphConditionalHandleCreate(&hL, graph, 1, cudaGraphCondAssignDefault));
+    gc = GraphCtl{};
+    gc.level = hL;
+    const int64_t l0 = launches;
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = hL;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t top;
+    try {
+      LV_CUDA(cudaGraphAddNode(&top, graph, nullptr, 0, &p));
+      cudaGraph_t level_body = p.conditional.phGraph_out[0];
+      LV_CUDA(cudaGraphConditionalHandleCreate(&hP, level_body, 0, 0));
+      LV_CUDA(cudaGraphConditionalHandleCreate(&hC, level_body, 0, 0));
+      gc.pass = hP;
+      gc.contract = hC;
+      gc.on = 1;
+      int64_t a = 0, b = 0, c = 0, d = 0, e = 0;
+      capture_into(level_body, cs[0], [&] {
+        k_gate_pass<<<1, 1, 0, st>>>(D, gc);
+        ++launches;
+        cudaGraph_t* pb = add_cond(st, hP, cudaGraphCondTypeWhile, 1);
+        a = launches;
+        capture_into(pb[0], cs[1], [&] { launch_pass<WI>(); });
+        k_pass = launches - a;
+        b = launches;
+        agg_prefix<WI>(-1);
+        k_gate_contract<<<1, 1, 0, st>>>(D, gc);
+        ++launches;
+        cudaGraph_t* cb = add_cond(st, hC, cudaGraphCondTypeIf, 2);
+        k_level = launches - b + 1;  // + k_gate_pass
+        LV_CUDA(cudaGraphConditionalHandleCreate(&hO, cb[0], 0, 0));
+        gc.ok = hO;
+        c = launches;
+        capture_into(cb[0], cs[1], [&] {
+          agg_contract_a<WI>();
+          k_gate_arena_agg<<<1, 1, 0, st>>>(D, gc);
+          ++launches;
+          cudaGraph_t* ob = add_cond(st, hO, cudaGraphCondTypeIf, 1);
+          k_contract = launches - c;
+          d = launches;
+          capture_into(ob[0], cs[2], [&] {
+            agg_contract_b<WI>();
+            agg_tail();
+            level_start_kernels();
+            k_gate_level<<<1, 1, 0, st>>>(D, gc);
+            ++launches;
+          });
+          k_ok = launches - d;
+        });
+        e = launches;
+        capture_into(cb[1], cs[1], [&] { agg_tail(); });
+        k_final = launches - e;
+      });
+      LV_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+    } catch (...) {
+      gc.on = 0;
+      launches = l0;
+      release_graph();
+      throw;
+    }
+    gc.on = 0;
+    launches = l0;
+    graph_arena = D.arena_keys;
+  }
+
+  // Waits for the stream, giving up (with an error; the work may still be running) after
+  // `seconds`. A captured run's loops end on device-side conditions, so the host bounds them.
+  void wait_bounded(double seconds) {
+    const auto t0 = std::chrono::steady_clock::now();
+    int spins = 0;
+    for (;;) {
+      const cudaError_t q = cudaStreamQuery(st);
+      if (q == cudaSuccess) return;
+      if (q != cudaErrorNotReady) LV_CUDA(q);
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > seconds)
+        throw Fail{LV_ERR_DEVICE_CHECK, "captured run did not finish within the time limit"};
+      if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+  }
+
+  struct SegCounts {
+    uint32_t levels, passes, aggs, contract, contract_ok, final_;
+  };
+  SegCounts seg_counts() {
+    return read_ctrl<SegCounts>(offsetof(Ctrl, seg_levels));
+  }
+
+  template <bool WI>
+  void louvain_graph() {
+    // the launch after a stop begins at a level start, which is where the host left the run
+    for (int launch = 0;; ++launch) {
+      if (!gexec || graph_arena != D.arena_keys) build_graph<WI>();
+      write_ctrl_u32(offsetof(Ctrl, abort), 0);
+      const SegCounts before = seg_counts();
+      LV_CUDA(cudaGraphLaunch(gexec, st));
+      ++graph_launches;
+      wait_bounded(600.0);
+      const SegCounts after = seg_counts();
+      // kernels that ran: the level body entry + aggregation prefix per level body, the pass
+      // body per pass, and each branch as often as it was taken (the gate counters)
+      launches += (int64_t)(after.passes - before.passes) * k_pass +
+                  (int64_t)(after.aggs - before.aggs) * k_level +
+                  (int64_t)(after.contract - before.contract) * k_contract +
+                  (int64_t)(after.contract_ok - before.contract_ok) * k_ok +
+                  (int64_t)(after.final_ - before.final_) * k_final;
+      check_device_errors();
+      const uint32_t ab = ctrl_u32(offsetof(Ctrl, abort));
+      if (ab == 0) break;
+      const unsigned long long need = read_ctrl<unsigned long long>(offsetof(Ctrl, abort_need));
+      ensure_arena(need);
+      if (ab == kAbortAggArena) {
+        // redo this level's aggregation with the host in charge, then continue captured
+        if (!aggregate(-1)) break;
+      }
+      if (launch > 64) throw Fail{LV_ERR_DEVICE_CHECK, "captured run kept stopping for arena growth"};
+    }
+    finished = true;
+    graph_mode_used = true;
+  }
+  bool graph_mode_used = false;
+  int64_t graph_launches = 0;
+
   // OptimizationPhase::run: passes until every graph of the batch has stopped its level.
   int32_t optimization_run() {
     int32_t passes = 0;
@@ -591,8 +885,12 @@ class Run {
     return passes;
   }
 
-  // modularity_routine's level loop.
+  // modularity_routine's level loop: captured and device-driven (use_graphs), or host-driven.
   void louvain() {
+    if (cfg.use_graphs && !debug && !finished) {
+      if (wint) louvain_graph<true>(); else louvain_graph<false>();
+      return;
+    }
     while (!finished) {
       optimization_run();
       aggregate(-1);
@@ -619,6 +917,19 @@ class Run {
     s->n = n0;
     s->m = m_edges;
     s->levels = levels_run;
+    if (graph_mode_used) {
+      // a captured run has no host events between its kernels: the device clock times them
+      unsigned long long t[3];
+      LV_CUDA(cudaMemcpyAsync(t, reinterpret_cast<char*>(D.ctrl) + offsetof(Ctrl, t_opt_ns), sizeof(t),
+                              cudaMemcpyDeviceToHost, st));
+      sync();
+      t_opt_ms = t[0] * 1e-6;
+      t_optk_ms = t[1] * 1e-6;
+      t_agg_ms = t[2] * 1e-6;
+      s->ms_optimization_kernels = (float)t_optk_ms;
+      s->levels = (int32_t)seg_counts().levels;
+    }
+    s->graph_launches = graph_launches;
     s->iterations = (int32_t)hs[0].total_iters;
     s->n_communities = (int32_t)hs[0].n_best;
     s->ms_optimization = (float)t_opt_ms;
@@ -685,7 +996,7 @@ void lv_config_default(lv_config* c) {
   c->chunk_edges = 50000000;        // STEP_ROUND
   c->weight_mode = LV_WEIGHTS_AUTO;
   c->validate = 1;
-  c->use_graphs = 1;
+  c->use_graphs = 0;
 }
 
 lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {

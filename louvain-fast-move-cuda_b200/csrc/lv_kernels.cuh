@@ -117,6 +117,7 @@ __device__ __forceinline__ bool has_nonloop(const Dev& D, uint32_t v, uint32_t d
 // of that chunk and of every later chunk are not considered in that pass.
 __global__ void k_chunk_flags(Dev D) {
   Ctrl* C = D.ctrl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) C->t_pass0 = global_ns();  // first kernel of a pass
   if (!C->chunk_on || !(C->fast || C->rule_sort)) return;
   const uint32_t n = C->n, it = C->it, nch = C->n_chunks;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
@@ -684,6 +685,8 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_apply(Dev D) {
   Ctrl* C = D.ctrl;
+  // the optimisation kernels of this pass ended when the first apply block starts
+  if (blockIdx.x == 0 && threadIdx.x == 0) C->t_optk_ns += global_ns() - C->t_pass0;
   const uint32_t count = C->mover_count, it = C->it;
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -833,7 +836,7 @@ __global__ void k_set_pass(Ctrl* C, uint32_t p, int mode, int fast_first) {
 // starting modularity instead (Community::update -> compute_modularity, community.h:57-65).
 template <bool WINT>
 __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts, int level_start,
-                                                   int mode, int fast_first) {
+                                                   int mode, int fast_first, GraphCtl gc) {
   Ctrl* C = D.ctrl;
   __shared__ double shd[33];
   __shared__ unsigned long long shu[33];
@@ -910,6 +913,11 @@ __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts
     } else {
       C->it += 1;
       C->pass += 1;
+      C->seg_passes += 1;
+      C->t_opt_ns += global_ns() - C->t_pass0;
+      if (C->seg_passes > kGuardPasses) atomicOr(&C->err, kErrLoop);
+      // the captured pass loop runs while a graph iterates (and no guard has tripped)
+      set_cond(gc, gc.pass, tot > 0 && !(C->err & kErrLoop));
     }
     set_pass_rule(C, C->pass, mode, fast_first);
   }
@@ -937,6 +945,7 @@ __global__ void k_level_init(Dev D) {
     C->apply_items = 0;
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
+    C->arena_need = 0;
     for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
   }
 }
@@ -1145,9 +1154,35 @@ __global__ void k_fill_gid(uint32_t* gid, const long long* offs, uint32_t G) {
   }
 }
 
+// Graphs uploaded one by one into a packed batch keep their local numbering; this rebases
+// them: row offsets of graph g gain its first entry eoffs[g], destinations its first vertex
+// voffs[g]. An entry finds its graph by binary search over eoffs (G is small).
+__global__ void k_rebase_pieces(long long* row64, uint32_t* col, const long long* voffs,
+                                const long long* eoffs, uint32_t G, uint32_t n, uint32_t E) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (uint32_t e = tid; e < E; e += nth) {
+    uint32_t lo = 0, hi = G;  // last g with eoffs[g] <= e
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((unsigned long long)eoffs[mid] <= e) lo = mid; else hi = mid;
+    }
+    col[e] += (uint32_t)voffs[lo];
+  }
+  for (uint32_t v = tid; v < n; v += nth) {
+    uint32_t lo = 0, hi = G;  // last g with voffs[g] <= v
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((unsigned long long)voffs[mid] <= v) lo = mid; else hi = mid;
+    }
+    row64[v] += eoffs[lo];
+  }
+  if (tid == 0) row64[n] = E;
+}
+
 // Hash-table arena needed by the global-table bin at this level: sum over vertices with
 // degree above the shared-memory bound of next_pow2(2 d).
-__global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap, unsigned long long* need) {
+__global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap) {
+  unsigned long long* need = &D.ctrl->arena_need;
   const uint32_t n = D.ctrl->n;
   unsigned long long s = 0;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
@@ -1297,7 +1332,6 @@ __global__ void k_hub_owner(Dev D, int bin) {
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     const uint32_t c0 = D.hub_off[idx] / kHubChunk;
     for (uint32_t j = threadIdx.x; j < cap / kHubChunk; j += blockDim.x) D.hub_owner[c0 + j] = s;
-    if (blockIdx.x == 0 && idx == 0 && threadIdx.x == 0) C->long_count = 0;
     if (threadIdx.x == 0) {
       D.newdeg[s] = 0;
       D.kB[s] = 0.0;
@@ -1392,14 +1426,20 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(Dev D) {
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   Acc* vals = reinterpret_cast<Acc*>(D.arena_vals);
   uint32_t err = 0;
+  const uint32_t n = C->n, n2 = C->n_next;
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
     const unsigned long long it = D.long_items[idx];
     const uint32_t v = (uint32_t)(it >> 32), piece = (uint32_t)it;
+    // an item always names a vertex of this level in a bin-7 community whose table fits the
+    // arena (k_hub_insert checked that when it queued the item); anything else is reported
+    if (v >= n) { err |= kErrIndex; continue; }
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     const uint32_t s = D.new_comm[v];
+    if (s >= n2) { err |= kErrIndex; continue; }
     const uint32_t off = D.hubtab[s];
     const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
+    if (off == kEmpty || (unsigned long long)off + cap > C->arena_slots) { err |= kErrIndex; continue; }
     const uint32_t mask = cap - 1u, shift = 32u - log2_pow2(cap);
     const uint32_t rs = D.row[v] + piece * kHubPiece;
     const uint32_t re = min(D.row[v + 1], rs + kHubPiece);
@@ -1421,7 +1461,8 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(Dev D) {
 // Bin-7 emit: one block per table chunk; occupied slots are appended to the community's row
 // (positions claimed with one atomic per block), k' and the self-loop weight accumulated.
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_hub_emit(Dev D, uint32_t nchunks) {
+__global__ void __launch_bounds__(512) k_hub_emit(Dev D) {
+  const uint32_t nchunks = min(D.ctrl->hub_cursor, D.ctrl->arena_slots) / kHubChunk;
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -1802,6 +1843,8 @@ __global__ void k_agg_finish(Dev D) {
     }
     C->n = n2;
     C->E = C->E_next;
+    C->seg_levels += 1;
+    C->t_agg_ns += global_ns() - C->t_agg0;
   }
 }
 
@@ -1809,6 +1852,10 @@ __global__ void k_agg_finish(Dev D) {
 // cont = Q_end - Q_level_start > threshold. force >= 0 overrides (phase-level API).
 __global__ void k_agg_decide(Dev D, int force, uint32_t max_levels) {
   Ctrl* C = D.ctrl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C->t_agg0 = global_ns();
+    C->seg_aggs += 1;
+  }
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
     GraphState* st = &D.gs[g];
     if (st->phase == kFinished) { st->agg = 0; continue; }
@@ -1822,14 +1869,94 @@ __global__ void k_agg_decide(Dev D, int force, uint32_t max_levels) {
   }
 }
 
+// ---- device-sized clears and the gates of a captured run ----------------------------------------
+// Aggregation scratch cleared to the level's own sizes (read on the device).
+__global__ void k_agg_clear_map(Dev D) {
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) D.map[i] = 0ull;
+}
+// Before the contraction: per-new-community counters and hub offsets, and the counters the
+// binning appends with (so that an aggregation can be run again from its start).
+__global__ void k_agg_clear_next(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t n2 = C->n_next;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n2; i += gridDim.x * blockDim.x) {
+    D.cd[i] = 0ull;
+    if (i < n2) D.hubtab[i] = kEmpty;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    D.newdeg[n2] = 0;
+    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    C->hub_cursor = 0;
+    C->long_count = 0;  // k_hub_insert queues this aggregation's long rows from zero
+  }
+}
+// The global contraction tables of this aggregation: empty keys, zero values.
+__global__ void k_arena_clear(Dev D) {
+  Ctrl* C = D.ctrl;
+  const uint32_t used = min(C->hub_cursor, C->arena_slots);
+  unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < used; s += gridDim.x * blockDim.x) {
+    D.arena_keys[s] = kEmpty;
+    vals[s] = 0ull;
+  }
+}
+// Level body entry: the pass loop runs while some graph iterates.
+__global__ void k_gate_pass(Dev D, GraphCtl gc) {
+  Ctrl* C = D.ctrl;
+  if (C->seg_aggs > kGuardLevels) atomicOr(&C->err, kErrLoop);
+  const bool stop = (C->err & kErrLoop) != 0;
+  set_cond(gc, gc.pass, C->n_iterating > 0 && !stop);
+  if (stop) set_cond(gc, gc.level, false);
+}
+// After the renumbering: contract (then-branch) when some graph continues, else the run ends.
+__global__ void k_gate_contract(Dev D, GraphCtl gc) {
+  Ctrl* C = D.ctrl;
+  const bool more = C->n_next > 0;
+  if (more) C->seg_contract += 1; else C->seg_final += 1;
+  const bool stop = (C->err & kErrLoop) != 0;
+  set_cond(gc, gc.contract, more && !stop);
+  if (!more || stop) set_cond(gc, gc.level, false);
+}
+// After the contraction binning: its global tables must fit the arena; if not, the run stops
+// here (nothing of this aggregation is final yet) and the host grows the arena and redoes it.
+__global__ void k_gate_arena_agg(Dev D, GraphCtl gc) {
+  Ctrl* C = D.ctrl;
+  const bool ok = C->hub_cursor <= C->arena_slots;
+  if (ok) {
+    C->seg_contract_ok += 1;
+  } else {
+    C->abort = kAbortAggArena;
+    C->abort_need = C->hub_cursor;
+    set_cond(gc, gc.level, false);
+  }
+  set_cond(gc, gc.ok, ok);
+}
+// End of a level start: the next level's optimisation tables must fit the arena; if not, the
+// run stops with the level started and the host grows the arena and resumes.
+__global__ void k_gate_level(Dev D, GraphCtl gc) {
+  Ctrl* C = D.ctrl;
+  const bool ok = C->arena_need <= C->arena_slots;
+  if (!ok) {
+    C->abort = kAbortOptArena;
+    C->abort_need = C->arena_need;
+  }
+  set_cond(gc, gc.level, ok && !(C->err & kErrLoop));
+}
+
 // ---- scans (3-phase: tile sums, scan of tile sums, tile scan + offset) ---------------------------
 constexpr int kScanNT = 256;
 constexpr int kScanIPT = 8;
 constexpr int kScanTile = kScanNT * kScanIPT;
 
+// Every scan takes its length either from the host (dn == nullptr) or from the device
+// (*dn + add, read when the kernel runs), so a captured sequence scans each level's size.
 template <class T>
-__global__ void __launch_bounds__(kScanNT) k_scan_tiles(const T* in, T* tile_sums, uint32_t n) {
+__global__ void __launch_bounds__(kScanNT) k_scan_tiles(const T* in, T* tile_sums, uint32_t n,
+                                                        const uint32_t* dn, uint32_t add) {
   __shared__ T sh[33];
+  if (dn) n = *dn + add;
+  if ((uint64_t)blockIdx.x * kScanTile >= n) return;
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
   T s = T(0);
 #pragma unroll
@@ -1843,8 +1970,10 @@ __global__ void __launch_bounds__(kScanNT) k_scan_tiles(const T* in, T* tile_sum
 }
 
 template <class T>
-__global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntiles) {
+__global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntiles,
+                                                    const uint32_t* dn, uint32_t add) {
   __shared__ T sh[33];
+  if (dn) ntiles = (*dn + add + kScanTile - 1) / kScanTile;
   // each thread scans a contiguous run, then the block scans the run totals
   const uint32_t per = (ntiles + 1023) / 1024;
   const uint32_t b = threadIdx.x * per, e = min(b + per, ntiles);
@@ -1863,8 +1992,10 @@ __global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntile
 // total_out != nullptr the grand total is written there.
 template <class T, bool INCLUSIVE>
 __global__ void __launch_bounds__(kScanNT) k_scan_apply(const T* in, T* out, const T* tile_offs,
-                                                         uint32_t n, T* total_out) {
+                                                         uint32_t n, const uint32_t* dn, uint32_t add) {
   __shared__ T sh[33];
+  if (dn) n = *dn + add;
+  if ((uint64_t)blockIdx.x * kScanTile >= n) return;
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanIPT;
   T vals[kScanIPT];
   T s = T(0);
@@ -1883,7 +2014,6 @@ __global__ void __launch_bounds__(kScanNT) k_scan_apply(const T* in, T* out, con
     if (j < n) out[j] = run;
     if (!INCLUSIVE) run += vals[i];
   }
-  if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == kScanNT - 1) *total_out = run;
 }
 
 }  // namespace lv

@@ -3,10 +3,12 @@
 //
 // Continuous batching with graph state resident in HBM: `max_slots` worker threads, each with
 // its own CUDA stream, take requests from a FIFO queue as soon as a slot is free and the
-// request's device footprint fits the memory budget next to the requests already running.
-// Each admitted request runs the full Louvain pipeline on its slot's stream, so requests
-// that arrive while others are on the GPU overlap with them on the device. Results stay on
-// the host until polled. The reference has no counterpart (it runs one graph per call).
+// requests' device footprint fits the memory budget next to the requests already running.
+// A slot takes the head of the queue together with the other queued small requests and runs
+// them as one packed batch (every graph of a batch gets exactly the result it gets alone);
+// batches on different slots overlap on the device, and device memory comes from the
+// context's pool, so steady-state serving allocates nothing. Results stay on the host until
+// polled. The reference has no counterpart (it runs one graph per call).
 #pragma once
 
 #include <chrono>
@@ -59,11 +61,22 @@ struct lv_server {
   bool stop = false;
   std::vector<std::thread> workers;
   std::vector<cudaStream_t> streams;
+  std::vector<uint32_t*> pinned;  // per slot: 64-byte readback buffer
+
+  // Continuous batching: a free slot takes the request at the head of the queue and, when
+  // that request is small, every further queued request (in arrival order) that is small too,
+  // of the same weight kind, fits the batch limits and fits the memory budget. The taken
+  // requests run as one packed batch on the slot's stream; requests that arrive meanwhile wait
+  // for the next free slot.
+  static constexpr int64_t kSmallEntries = 1 << 22;   // requests up to 4M CSR entries batch
+  static constexpr int64_t kBatchEntries = 1 << 24;   // at most 16M entries per batch
+  static constexpr size_t kBatchGraphs = 1024;
 
   void worker(int slot) {
     cudaSetDevice(ctx->device);
+    std::vector<lv::Request*> batch;
     for (;;) {
-      lv::Request* r = nullptr;
+      batch.clear();
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] {
@@ -71,53 +84,94 @@ struct lv_server {
         });
         if (stop && queue.empty()) return;
         if (queue.empty() || used_bytes + (int64_t)queue.front()->est_bytes > budget) continue;
-        r = queue.front();
+        lv::Request* r0 = queue.front();
         queue.pop_front();
-        r->state = 1;
-        used_bytes += (int64_t)r->est_bytes;
-        ++n_running;
+        batch.push_back(r0);
+        used_bytes += (int64_t)r0->est_bytes;
+        // a graph batches only while one edge chunk covers it (the chunk rule of a single run
+        // then never splits its pass, so the batch result is the single-run result)
+        const int64_t chunk = ctx->cfg.chunk_edges > 0 ? ctx->cfg.chunk_edges : kSmallEntries;
+        const int64_t small = std::min<int64_t>(kSmallEntries, chunk);
+        if (r0->E <= small) {
+          int64_t entries = r0->E;
+          for (auto it = queue.begin(); it != queue.end() && batch.size() < kBatchGraphs;) {
+            lv::Request* r = *it;
+            if (r->E <= small && r->weighted == r0->weighted &&
+                entries + r->E <= kBatchEntries && used_bytes + (int64_t)r->est_bytes <= budget) {
+              batch.push_back(r);
+              entries += r->E;
+              used_bytes += (int64_t)r->est_bytes;
+              it = queue.erase(it);
+            } else {
+              ++it;
+            }
+          }
+        }
+        for (lv::Request* r : batch) r->state = 1;
+        n_running += (int64_t)batch.size();
       }
-      run_one(r, slot);
+      run_batch(batch, slot);
       {
         std::lock_guard<std::mutex> lk(mu);
-        used_bytes -= (int64_t)r->est_bytes;
-        --n_running;
-        ++n_done;
-        r->state = 2;
-        r->t_done = std::chrono::steady_clock::now();
-        // the request's input is no longer needed
-        std::vector<int64_t>().swap(r->row);
-        std::vector<int32_t>().swap(r->col);
-        std::vector<float>().swap(r->w);
+        const auto now = std::chrono::steady_clock::now();
+        for (lv::Request* r : batch) {
+          used_bytes -= (int64_t)r->est_bytes;
+          r->state = 2;
+          r->t_done = now;
+          // the request's input is no longer needed
+          std::vector<int64_t>().swap(r->row);
+          std::vector<int32_t>().swap(r->col);
+          std::vector<float>().swap(r->w);
+          r->brow = nullptr;
+          r->bcol = nullptr;
+          r->bw = nullptr;
+        }
+        n_running -= (int64_t)batch.size();
+        n_done += (int64_t)batch.size();
       }
       cv_work.notify_all();
       cv_done.notify_all();
     }
   }
 
-  void run_one(lv::Request* r, int slot) {
+  void run_batch(const std::vector<lv::Request*>& batch, int slot) {
     try {
-      lv::Run run(ctx, streams[slot]);
-      const bool borrowed = r->brow != nullptr;
-      run.init(1, nullptr, r->n, borrowed ? r->brow : r->row.data(), borrowed ? r->bcol : r->col.data(),
-               r->weighted ? (borrowed ? r->bw : r->w.data()) : nullptr, LV_MEM_HOST);
+      lv::Run run(ctx, streams[slot], pinned[slot]);
+      std::vector<lv::Run::Piece> ps;
+      ps.reserve(batch.size());
+      for (lv::Request* r : batch) {
+        const bool b = r->brow != nullptr;
+        ps.push_back({r->n, r->E, b ? r->brow : r->row.data(), b ? r->bcol : r->col.data(),
+                      r->weighted ? (b ? r->bw : r->w.data()) : nullptr});
+      }
+      run.init_pieces(ps);
       run.louvain();
-      r->out.resize((size_t)r->n);
-      lv::GraphState gs;
-      cudaError_t e = cudaMemcpyAsync(r->out.data(), run.D.out, (size_t)r->n * 4, cudaMemcpyDeviceToHost, run.st);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(&gs, run.D.gs, sizeof(gs), cudaMemcpyDeviceToHost, run.st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(run.st);
-      if (e != cudaSuccess) throw lv::Fail{LV_ERR_CUDA, cudaGetErrorString(e)};
-      r->modularity = gs.Q;
-      r->n_comm = (int32_t)gs.n_best;
-      r->status = LV_OK;
+      std::vector<lv::GraphState> gs(batch.size());
+      int64_t vb = 0;
+      for (lv::Request* r : batch) {
+        r->out.resize((size_t)r->n);
+        LV_CUDA(cudaMemcpyAsync(r->out.data(), run.D.out + vb, (size_t)r->n * 4, cudaMemcpyDeviceToHost, run.st));
+        vb += r->n;
+      }
+      LV_CUDA(cudaMemcpyAsync(gs.data(), run.D.gs, sizeof(lv::GraphState) * batch.size(),
+                              cudaMemcpyDeviceToHost, run.st));
+      LV_CUDA(cudaStreamSynchronize(run.st));
+      for (size_t i = 0; i < batch.size(); ++i) {
+        batch[i]->modularity = gs[i].Q;
+        batch[i]->n_comm = (int32_t)gs[i].n_best;
+        batch[i]->status = LV_OK;
+      }
     } catch (const lv::Fail& f) {
-      r->status = f.st;
-      r->err = f.msg;
+      for (lv::Request* r : batch) {
+        r->status = f.st;
+        r->err = f.msg;
+      }
       cudaGetLastError();
     } catch (const std::bad_alloc&) {
-      r->status = LV_ERR_NOMEM;
-      r->err = "host allocation failed";
+      for (lv::Request* r : batch) {
+        r->status = LV_ERR_NOMEM;
+        r->err = "host allocation failed";
+      }
     }
   }
 };
@@ -140,6 +194,14 @@ lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_sl
       return LV_ERR_CUDA;
     }
     s->streams.push_back(st);
+    uint32_t* pb = nullptr;
+    if (cudaMallocHost(&pb, 64) != cudaSuccess) {
+      for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+      for (uint32_t* x : s->pinned) cudaFreeHost(x);
+      cudaGetLastError();
+      return LV_ERR_CUDA;
+    }
+    s->pinned.push_back(pb);
   }
   lv_server* p = s.get();
   for (int i = 0; i < max_slots; ++i) s->workers.emplace_back([p, i] { p->worker(i); });
@@ -163,6 +225,7 @@ lv_status lv_server_destroy(lv_server* s) {
   s->cv_work.notify_all();
   for (auto& t : s->workers) t.join();
   for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+  for (uint32_t* pb : s->pinned) cudaFreeHost(pb);
   delete s;
   return LV_OK;
 }
@@ -171,6 +234,7 @@ static lv_status server_submit(lv_server* s, int64_t n, const int64_t* row_ptr, 
                                const float* w, bool borrow, int64_t* request_id) {
   if (!s || !row_ptr || !col || !request_id || n <= 0) return LV_ERR_ARGUMENT;
   const int64_t E = row_ptr[n];
+  if (row_ptr[0] != 0) return LV_ERR_INPUT;
   if (E <= 0 || E > (1ll << 30)) return LV_ERR_RANGE;
   auto r = std::make_unique<lv::Request>();
   r->n = n;
