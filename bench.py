@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--pool", type=int, default=64, help="served: distinct request graphs")
     ap.add_argument("--slots", type=int, default=16, help="served: concurrent server slots")
     ap.add_argument("--rates", default="10,50,200,1000,2000", help="served: arrival rates, req/s")
+    ap.add_argument("--captured", type=int, default=-1, choices=[-1, 0, 1],
+                    help="1: run the level loop as one captured CUDA graph, 0: host-driven, "
+                         "-1: the library default")
     return ap.parse_args()
 
 
@@ -324,7 +327,8 @@ def run_served(args, local):
         keep.append((rp, cl))
         pool.append(graphs.CSRGraph(n=g.n, row_ptr=rp.numpy(), col=cl.numpy(), w=None, name=g.name))
     torch.cuda.empty_cache()
-    eng = lv.Engine(local)
+    kw = {} if args.captured < 0 else {"use_graphs": bool(args.captured)}
+    eng = lv.Engine(local, **kw)
     # loop baseline: the pool once, one call per request, host buffers in and out
     for g in pool[:4]:
         eng.run_graph(g)
@@ -410,7 +414,8 @@ def main():
     torch.cuda.set_device(local)
     g = build_graph(args.scale, device=dev)
     mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
-    eng = lv.Engine(local, mode=mode)
+    kw = {} if args.captured < 0 else {"use_graphs": bool(args.captured)}
+    eng = lv.Engine(local, mode=mode, **kw)
 
     row_d = torch.from_numpy(g.row_ptr).to(dev)
     col_d = torch.from_numpy(g.col).to(dev)

@@ -76,8 +76,9 @@ typedef struct {
   int32_t validate;         /* 1 = check row_ptr monotone / col in range / no empty row on
                                the device before running (default 1) */
   int32_t use_graphs;       /* 1 = run the level loop (passes, aggregation, next level) as one
-                               captured CUDA graph with device-side loop control;
-                               0 = host-driven, one stream launch sequence per pass (default) */
+                               captured CUDA graph with device-side loop control, captured once
+                               per context (or serving slot) and replayed (default);
+                               0 = host-driven, one stream launch sequence per pass */
   int32_t reserved_i[7];
   /* degree-bin tiling; 0 = use the autotuned or built-in table */
   int32_t bin_max_degree[8];
@@ -221,7 +222,9 @@ lv_status lv_modularity_noalloc(int64_t n, const int64_t* row_ptr, const int32_t
 /* ---- serving ---------------------------------------------------------------------------
  * Continuous batching with graph state resident in HBM. No reference counterpart.
  * Requests are admitted while the device memory they need fits `budget_bytes` and a slot is
- * free; admitted requests run concurrently on their own streams. */
+ * free (1 <= max_slots <= 64); a free slot takes the request at the head of the queue and the
+ * other queued small requests (up to 4M entries each) as one batch, and slots run concurrently
+ * on their own streams. With cfg.use_graphs each slot replays one captured level loop. */
 typedef struct lv_server lv_server;
 lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_slots,
                            lv_server** out);

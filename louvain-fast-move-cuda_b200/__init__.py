@@ -176,7 +176,7 @@ def _is_device(a) -> bool:
 def config(mode: int = MODE.SORT, threshold: float = 1e-3, fast_first: bool = True,
            chunk_edges: int = 50_000_000, max_iterations: int = 1_000_000_000,
            max_levels: int = 0, weight_mode: int = WEIGHTS_AUTO,
-           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = False) -> Config:
+           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = True) -> Config:
     c = Config()
     load_library().lv_config_default(ctypes.byref(c))
     c.mode = int(mode)

@@ -25,9 +25,69 @@
 #include "../../include/louvain_b200.h"
 #include "lv_kernels.cuh"
 
+namespace lv {
+
+// Everything that fixes the kernel sequence of a captured run apart from the data: when two
+// runs agree on it, the second reuses the first one's instantiated graph.
+struct GraphKey {
+  int32_t wint, single, mode, fast_first, max_levels, sms, grid_n, grid_sq, grid_block;
+  int64_t chunk_edges;
+  uint32_t maxdeg[kNumBins], block_cap, team_cap[6];
+  int32_t grid_team[6];
+};
+
+// A fixed c_dev entry for a run's Dev (the pointer table every kernel reads; kernels take the
+// entry's index) and the captured level loop built against it. A context has one, each serving
+// slot has one; whichever run uses the slot writes its own Dev there first, so the instantiated
+// graph serves every run of the same GraphKey without being captured again.
+// Slot indices into c_dev, shared by every context and server of the process.
+static std::mutex g_slot_mu;
+static bool g_slot_used[kMaxDevSlots] = {};
+
+struct DevSlot {
+  int id = -1;                  // index into c_dev
+  const void* owner = nullptr;  // the run whose Dev is in c_dev[id]
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  GraphKey key{};
+  GraphCtl gc{};
+  int64_t k_pass = 0, k_level = 0, k_contract = 0, k_ok = 0, k_final = 0;  // kernels per segment
+  cudaStream_t cs[3] = {nullptr, nullptr, nullptr};  // capture streams of nested bodies
+
+  cudaError_t create() {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (int i = 0; i < kMaxDevSlots; ++i)
+      if (!g_slot_used[i]) {
+        g_slot_used[i] = true;
+        id = i;
+        return cudaSuccess;
+      }
+    return cudaErrorMemoryAllocation;
+  }
+  void release_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  void destroy() {
+    release_graph();
+    for (auto& x : cs)
+      if (x) cudaStreamDestroy(x);
+    if (id >= 0) {
+      std::lock_guard<std::mutex> lk(g_slot_mu);
+      g_slot_used[id] = false;
+    }
+    id = -1;
+  }
+};
+
+}  // namespace lv
+
 // A context keeps the device memory of finished runs in a pool and hands it to the next run,
 // so repeated calls allocate nothing (cudaMalloc / cudaFree synchronise the whole device).
 struct lv_context {
+  lv::DevSlot slot;  // the Dev buffer and captured graph of runs on `stream`
   int device = 0;
   lv_config cfg{};
   int sms = 148;
@@ -182,21 +242,35 @@ class Run {
   bool debug = std::getenv("LV_DEBUG") != nullptr;  // per-level sizes and bin populations on stderr
   cudaEvent_t ev[6];
   std::vector<Block> arena_blocks;
+  DevSlot* slot = nullptr;
+  int Dd = -1;           // the slot whose c_dev entry kernels read D from
+  bool dev_dirty = true;
+
+  // Makes the slot's c_dev entry this run's D (after any change of D, and whenever another run
+  // used the slot in between). Stream-ordered, so kernels launched afterwards see it.
+  void bind() {
+    if (slot->owner == this && !dev_dirty) return;
+    LV_CUDA(cudaMemcpyToSymbolAsync(c_dev, &D, sizeof(Dev), (size_t)Dd * sizeof(Dev),
+                                    cudaMemcpyHostToDevice, st));
+    slot->owner = this;
+    dev_dirty = false;
+  }
 
   // stream == nullptr: the context's stream and readback buffer (calls serialised by the
   // context lock); otherwise a private stream, as the serving loop runs several at once, with
   // the caller's 64-byte pinned readback buffer (or one of the run's own if none is given).
-  explicit Run(lv_context* c, cudaStream_t stream = nullptr, uint32_t* pinned_buf = nullptr)
+  explicit Run(lv_context* c, cudaStream_t stream = nullptr, uint32_t* pinned_buf = nullptr,
+               DevSlot* dslot = nullptr)
       : ctx(c), cfg(c->cfg) {
     for (auto& e : ev) e = nullptr;
     st = stream ? stream : c->stream;
     pinned = stream ? pinned_buf : c->pinned;
+    slot = dslot ? dslot : &c->slot;
+    Dd = slot->id;
   }
   ~Run() {
     cudaStreamSynchronize(st);
-    release_graph();
-    for (cudaStream_t x : cs)
-      if (x) cudaStreamDestroy(x);
+    if (slot->owner == this) slot->owner = nullptr;
     for (const Block& b : owned) ctx->give(b.p, b.bytes);
     for (const Block& b : arena_blocks) ctx->give(b.p, b.bytes);
     if (own_pinned && pinned) cudaFreeHost(pinned);
@@ -405,8 +479,9 @@ class Run {
       D.gidB = dalloc<uint32_t>(ctx, owned, n);
       D.gid0 = dalloc<uint32_t>(ctx, owned, n0);
     }
-    scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2);
-    scan_tot = dalloc<unsigned long long>(ctx, owned, 1);
+    D.scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2);
+    dev_dirty = true;
+    bind();
   }
 
   // Integer or float semantics (the weights, if any, are already in D.w), then the bin tables.
@@ -455,44 +530,39 @@ class Run {
     }
     const float* wf = weighted ? reinterpret_cast<const float*>(D.w) : nullptr;
     iota_best();
-    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(D, row64(), wf, n, E);
-    else k_prep<false><<<grid_n, 256, 0, st>>>(D, row64(), wf, n, E);
-    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(D, wf);
-    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(D, wf);
-    if (wint) k_prep_total<true><<<1, 256, 0, st>>>(D);
-    else k_prep_total<false><<<1, 256, 0, st>>>(D);
+    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, n, E);
+    else k_prep<false><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, n, E);
+    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf);
+    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf);
+    if (wint) k_prep_total<true><<<1, 256, 0, st>>>(Dd);
+    else k_prep_total<false><<<1, 256, 0, st>>>(Dd);
     launches += 4;
     check_device_errors();
     level_start();
   }
 
  public:
-  unsigned long long* scan_tmp = nullptr;
-  unsigned long long* scan_tot = nullptr;
 
   void iota_best();
 
   // ---- scans --------------------------------------------------------------------------------
-  template <class T, bool INCL>
-  void scan(const T* in, T* out, uint32_t count, const uint32_t* dcount = nullptr, uint32_t add = 0) {
-    // count: the length (dcount == nullptr) or an upper bound of *dcount + add (the grid)
-    if (count == 0) return;
-    const uint32_t tiles = (count + kScanTile - 1) / kScanTile;
-    T* tmp = reinterpret_cast<T*>(scan_tmp);
-    k_scan_tiles<T><<<tiles, kScanNT, 0, st>>>(in, tmp, count, dcount, add);
-    k_scan_sums<T><<<1, 1024, 0, st>>>(tmp, tiles, dcount, add);
-    k_scan_apply<T, INCL><<<tiles, kScanNT, 0, st>>>(in, out, tmp, count, dcount, add);
+  template <class T, bool INCL, int SRC>
+  void scan() {
+    const int grid = ctx->sms * 4;
+    k_scan_tiles<T, SRC><<<grid, kScanNT, 0, st>>>(Dd);
+    k_scan_sums<T, SRC><<<1, 1024, 0, st>>>(Dd);
+    k_scan_apply<T, SRC, INCL><<<grid, kScanNT, 0, st>>>(Dd);
     launches += 3;
   }
 
   // ---- level start ------------------------------------------------------------------------------
   void commit_sq() {
-    if (wint) k_commit_sq<true><<<grid_sq, 256, 0, st>>>(D, single() ? 1 : 0);
-    else k_commit_sq<false><<<grid_sq, 256, 0, st>>>(D, single() ? 1 : 0);
+    if (wint) k_commit_sq<true><<<grid_sq, 256, 0, st>>>(Dd, single() ? 1 : 0);
+    else k_commit_sq<false><<<grid_sq, 256, 0, st>>>(Dd, single() ? 1 : 0);
   }
   void finalize(int level_start_flag) {
-    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
-    else k_finalize<false><<<1, 1024, 0, st>>>(D, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
+    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
+    else k_finalize<false><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
   }
 
   void ensure_arena(uint64_t need_slots) {
@@ -511,19 +581,21 @@ class Run {
     D.arena_vals = dalloc<unsigned long long>(ctx, arena_blocks, slots);
     D.hub_owner = dalloc<uint32_t>(ctx, arena_blocks, slots / kHubChunk + 1);
     arena_slots = slots;
+    dev_dirty = true;
+    bind();
     write_ctrl_u32(offsetof(Ctrl, arena_slots), (uint32_t)slots);
   }
 
   // Community::update at a new level, then the arena the level's global tables need.
   void level_start_kernels() {
     if (single() && cfg.chunk_edges > 0) {
-      k_chunk_bounds<<<1, 1, 0, st>>>(D, (unsigned long long)cfg.chunk_edges);
+      k_chunk_bounds<<<1, 1, 0, st>>>(Dd, (unsigned long long)cfg.chunk_edges);
       ++launches;
     }
-    k_level_init<<<grid_n, 256, 0, st>>>(D);
+    k_level_init<<<grid_n, 256, 0, st>>>(Dd);
     commit_sq();
     finalize(1);
-    k_arena_need<<<grid_n, 256, 0, st>>>(D, bins.maxdeg[6], bins.block_cap);
+    k_arena_need<<<grid_n, 256, 0, st>>>(Dd, bins.maxdeg[6], bins.block_cap);
     launches += 4;
   }
   void level_start() {
@@ -537,23 +609,23 @@ class Run {
   void launch_pass() {
     const size_t slot = 4 + (WI ? 4 : 8);
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
-    k_chunk_flags<<<grid_n, 256, 0, st>>>(D);
-    k_bin_vertices<<<grid_n, 256, 0, st>>>(D, bins);
-    k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
-    k_opt_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
-    k_opt_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
-    k_opt_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
-    k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
-    k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
-    k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
+    k_chunk_flags<<<grid_n, 256, 0, st>>>(Dd);
+    k_bin_vertices<<<grid_n, 256, 0, st>>>(Dd, bins);
+    k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(Dd, 0, team_cap[0]);
+    k_opt_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
+    k_opt_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
+    k_opt_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
+    k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
+    k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
+    k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
-    k_opt_hub_prep<<<ctx->sms * 4, 256, 0, st>>>(D);
-    k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
-    k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
-    k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(D);
+    k_opt_hub_prep<<<ctx->sms * 4, 256, 0, st>>>(Dd);
+    k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(Dd);
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[5], st));
-    k_apply<WI><<<grid_n, 256, 0, st>>>(D);
-    k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(D);
+    k_apply<WI><<<grid_n, 256, 0, st>>>(Dd);
+    k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
     commit_sq();
     finalize(0);
     launches += 17;
@@ -587,51 +659,49 @@ class Run {
   // the arena check and let the host redo the aggregation with a larger arena.
   template <bool WI>
   void agg_prefix(int force) {
-    const uint32_t gb = std::max<uint32_t>(1, (G + 255) / 256);
-    k_agg_decide<<<gb, 256, 0, st>>>(D, force, (uint32_t)std::max(0, cfg.max_levels));
-    k_agg_clear_map<<<grid_n, 256, 0, st>>>(D);
-    k_agg_mark<<<grid_n, 256, 0, st>>>(D);
-    k_agg_flags<<<grid_n, 256, 0, st>>>(D);
-    scan<unsigned long long, true>(D.map, D.map, scan_bound(), &D.ctrl->n, 0);
-    k_agg_meta<<<gb, 256, 0, st>>>(D);
+    const uint32_t gb = 32;  // grid-stride over graphs; fixed so that captured graphs are reusable
+    k_agg_decide<<<gb, 256, 0, st>>>(Dd, force, (uint32_t)std::max(0, cfg.max_levels));
+    k_agg_clear_map<<<grid_n, 256, 0, st>>>(Dd);
+    k_agg_mark<<<grid_n, 256, 0, st>>>(Dd);
+    k_agg_flags<<<grid_n, 256, 0, st>>>(Dd);
+    scan<unsigned long long, true, kScanMap>();
+    k_agg_meta<<<gb, 256, 0, st>>>(Dd);
     launches += 5;
   }
   template <bool WI>
   void agg_contract_a() {
-    k_agg_clear_next<<<grid_n, 256, 0, st>>>(D);
-    k_agg_count<<<grid_n, 256, 0, st>>>(D);
-    scan<unsigned long long, false>(D.cd, D.cd, scan_bound() + 1, &D.ctrl->n_next, 1);
-    k_agg_scatter<<<grid_n, 256, 0, st>>>(D);
-    k_agg_bin<<<grid_n, 256, 0, st>>>(D, bins);
+    k_agg_clear_next<<<grid_n, 256, 0, st>>>(Dd);
+    k_agg_count<<<grid_n, 256, 0, st>>>(Dd);
+    scan<unsigned long long, false, kScanCd>();
+    k_agg_scatter<<<grid_n, 256, 0, st>>>(Dd);
+    k_agg_bin<<<grid_n, 256, 0, st>>>(Dd, bins);
     launches += 4;
   }
   template <bool WI>
   void agg_contract_b() {
     const size_t slot = 4 + (WI ? 4 : 8);
     // the largest new communities: many blocks insert into their global tables
-    k_arena_clear<<<ctx->sms * 8, 256, 0, st>>>(D);
-    k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(D, kNumBins - 1);
-    k_hub_insert<WI><<<grid_n, 256, 0, st>>>(D);
-    k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(D);
-    k_hub_emit<WI><<<ctx->sms * 8, 512, 0, st>>>(D);
-    k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(D, 0, team_cap[0]);
-    k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(D, 1, team_cap[1]);
-    k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(D, 2, team_cap[2]);
-    k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(D, 3, team_cap[3]);
-    k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(D, 4, team_cap[4]);
-    k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(D, 5, team_cap[5]);
-    k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(D, 6, block_cap);
-    scan<uint32_t, false>(D.newdeg, D.rowB, scan_bound() + 1, &D.ctrl->n_next, 1);
-    k_agg_compact<WI><<<grid_n, 256, 0, st>>>(D);
+    k_arena_clear<<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(Dd, kNumBins - 1);
+    k_hub_insert<WI><<<grid_n, 256, 0, st>>>(Dd);
+    k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    k_hub_emit<WI><<<ctx->sms * 8, 512, 0, st>>>(Dd);
+    k_contract_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(Dd, 0, team_cap[0]);
+    k_contract_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
+    k_contract_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
+    k_contract_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
+    k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
+    k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
+    k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
+    scan<uint32_t, false, kScanDeg>();
+    k_agg_compact<WI><<<grid_n, 256, 0, st>>>(Dd);
     launches += 13;
   }
   void agg_tail() {
-    k_agg_best<<<grid_n, 256, 0, st>>>(D);
-    k_agg_finish<<<grid_n, 256, 0, st>>>(D);
+    k_agg_best<<<grid_n, 256, 0, st>>>(Dd);
+    k_agg_finish<<<grid_n, 256, 0, st>>>(Dd);
     launches += 2;
   }
-  // Scan grids: exact level sizes when the host drives, level-0 sizes in a captured run.
-  uint32_t scan_bound() const { return gc.on ? n0 : n; }
 
   // Returns true if any graph continues to a new level.
   template <bool WI>
@@ -685,18 +755,28 @@ class Run {
   // A launch runs every remaining level of every graph without a host round trip. It stops
   // early only when a level needs a larger hash-table arena (Ctrl::abort says which); the host
   // then grows the arena and continues, re-capturing because the arena pointers changed.
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  void* graph_arena = nullptr;  // arena the graph was captured with
-  GraphCtl gc{};
-  cudaStream_t cs[3] = {nullptr, nullptr, nullptr};
-  int64_t k_pass = 0, k_level = 0, k_contract = 0, k_ok = 0, k_final = 0;  // kernels per segment
+  GraphCtl gc{};  // handles while capturing (on = 1 only then); launches read it by value
 
-  void release_graph() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (graph) cudaGraphDestroy(graph);
-    gexec = nullptr;
-    graph = nullptr;
+  GraphKey graph_key() const {
+    GraphKey k;
+    std::memset(&k, 0, sizeof(k));
+    k.wint = wint;
+    k.single = single();
+    k.mode = cfg.mode;
+    k.fast_first = cfg.fast_first;
+    k.max_levels = cfg.max_levels;
+    k.sms = ctx->sms;
+    k.grid_n = grid_n;
+    k.grid_sq = grid_sq;
+    k.grid_block = grid_block[0];
+    k.chunk_edges = single() ? cfg.chunk_edges : 0;
+    for (int b = 0; b < kNumBins; ++b) k.maxdeg[b] = bins.maxdeg[b];
+    k.block_cap = bins.block_cap;
+    for (int b = 0; b < 6; ++b) {
+      k.team_cap[b] = team_cap[b];
+      k.grid_team[b] = grid_team[b];
+    }
+    return k;
   }
 
   // Adds a conditional node after the work captured so far on `s` and returns its body graphs.
@@ -741,10 +821,13 @@ class Run {
 
   template <bool WI>
   void build_graph() {
-    release_graph();
-    for (auto& x : cs)
+    slot->release_graph();
+    for (auto& x : slot->cs)
       if (!x) LV_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    cudaStream_t* cs = slot->cs;
+    cudaGraph_t graph = nullptr;
     LV_CUDA(cudaGraphCreate(&graph, 0));
+    slot->graph = graph;
     // each handle belongs to the graph that holds its conditional node; only the level loop's
     // handle has a launch default (1), the others are set by a gate kernel before their node
     cudaGraphConditionalHandle hL, hP, hC, hO;
@@ -768,51 +851,52 @@ class Run {
       gc.on = 1;
       int64_t a = 0, b = 0, c = 0, d = 0, e = 0;
       capture_into(level_body, cs[0], [&] {
-        k_gate_pass<<<1, 1, 0, st>>>(D, gc);
+        k_gate_pass<<<1, 1, 0, st>>>(Dd, gc);
         ++launches;
         cudaGraph_t* pb = add_cond(st, hP, cudaGraphCondTypeWhile, 1);
         a = launches;
         capture_into(pb[0], cs[1], [&] { launch_pass<WI>(); });
-        k_pass = launches - a;
+        slot->k_pass = launches - a;
         b = launches;
         agg_prefix<WI>(-1);
-        k_gate_contract<<<1, 1, 0, st>>>(D, gc);
+        k_gate_contract<<<1, 1, 0, st>>>(Dd, gc);
         ++launches;
         cudaGraph_t* cb = add_cond(st, hC, cudaGraphCondTypeIf, 2);
-        k_level = launches - b + 1;  // + k_gate_pass
+        slot->k_level = launches - b + 1;  // + k_gate_pass
         LV_CUDA(cudaGraphConditionalHandleCreate(&hO, cb[0], 0, 0));
         gc.ok = hO;
         c = launches;
         capture_into(cb[0], cs[1], [&] {
           agg_contract_a<WI>();
-          k_gate_arena_agg<<<1, 1, 0, st>>>(D, gc);
+          k_gate_arena_agg<<<1, 1, 0, st>>>(Dd, gc);
           ++launches;
           cudaGraph_t* ob = add_cond(st, hO, cudaGraphCondTypeIf, 1);
-          k_contract = launches - c;
+          slot->k_contract = launches - c;
           d = launches;
           capture_into(ob[0], cs[2], [&] {
             agg_contract_b<WI>();
             agg_tail();
             level_start_kernels();
-            k_gate_level<<<1, 1, 0, st>>>(D, gc);
+            k_gate_level<<<1, 1, 0, st>>>(Dd, gc);
             ++launches;
           });
-          k_ok = launches - d;
+          slot->k_ok = launches - d;
         });
         e = launches;
         capture_into(cb[1], cs[1], [&] { agg_tail(); });
-        k_final = launches - e;
+        slot->k_final = launches - e;
       });
-      LV_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+      LV_CUDA(cudaGraphInstantiate(&slot->exec, graph, 0));
     } catch (...) {
       gc.on = 0;
       launches = l0;
-      release_graph();
+      slot->release_graph();
       throw;
     }
+    slot->gc = gc;
+    slot->key = graph_key();
     gc.on = 0;
     launches = l0;
-    graph_arena = D.arena_keys;
   }
 
   // Waits for the stream, giving up (with an error; the work may still be running) after
@@ -826,7 +910,8 @@ class Run {
       if (q != cudaErrorNotReady) LV_CUDA(q);
       if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > seconds)
         throw Fail{LV_ERR_DEVICE_CHECK, "captured run did not finish within the time limit"};
-      if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(200));
+      // spin first (short runs finish in well under a millisecond), then yield the core
+      if (++spins > 4096) std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
   }
 
@@ -836,34 +921,46 @@ class Run {
   SegCounts seg_counts() {
     return read_ctrl<SegCounts>(offsetof(Ctrl, seg_levels));
   }
+  // Ctrl from `abort` to the segment counters, read back in one copy after a launch.
+  struct LaunchEnd {
+    uint32_t abort, pad;
+    unsigned long long arena_need, abort_need;
+    SegCounts seg;
+  };
+  static_assert(offsetof(Ctrl, seg_levels) - offsetof(Ctrl, abort) == offsetof(LaunchEnd, seg),
+                "LaunchEnd mirrors Ctrl");
+  static_assert(sizeof(LaunchEnd) <= 64, "fits the pinned readback buffer");
 
   template <bool WI>
   void louvain_graph() {
+    SegCounts prev = seg_counts();
+    bool reset_abort = false;
     // the launch after a stop begins at a level start, which is where the host left the run
     for (int launch = 0;; ++launch) {
-      if (!gexec || graph_arena != D.arena_keys) build_graph<WI>();
-      write_ctrl_u32(offsetof(Ctrl, abort), 0);
-      const SegCounts before = seg_counts();
-      LV_CUDA(cudaGraphLaunch(gexec, st));
+      const GraphKey key = graph_key();
+      if (!slot->exec || std::memcmp(&key, &slot->key, sizeof(key)) != 0) build_graph<WI>();
+      bind();
+      if (reset_abort) write_ctrl_u32(offsetof(Ctrl, abort), 0);
+      LV_CUDA(cudaGraphLaunch(slot->exec, st));
       ++graph_launches;
       wait_bounded(600.0);
-      const SegCounts after = seg_counts();
+      const LaunchEnd end = read_ctrl<LaunchEnd>(offsetof(Ctrl, abort));
       // kernels that ran: the level body entry + aggregation prefix per level body, the pass
       // body per pass, and each branch as often as it was taken (the gate counters)
-      launches += (int64_t)(after.passes - before.passes) * k_pass +
-                  (int64_t)(after.aggs - before.aggs) * k_level +
-                  (int64_t)(after.contract - before.contract) * k_contract +
-                  (int64_t)(after.contract_ok - before.contract_ok) * k_ok +
-                  (int64_t)(after.final_ - before.final_) * k_final;
+      launches += (int64_t)(end.seg.passes - prev.passes) * slot->k_pass +
+                  (int64_t)(end.seg.aggs - prev.aggs) * slot->k_level +
+                  (int64_t)(end.seg.contract - prev.contract) * slot->k_contract +
+                  (int64_t)(end.seg.contract_ok - prev.contract_ok) * slot->k_ok +
+                  (int64_t)(end.seg.final_ - prev.final_) * slot->k_final;
       check_device_errors();
-      const uint32_t ab = ctrl_u32(offsetof(Ctrl, abort));
-      if (ab == 0) break;
-      const unsigned long long need = read_ctrl<unsigned long long>(offsetof(Ctrl, abort_need));
-      ensure_arena(need);
-      if (ab == kAbortAggArena) {
+      if (end.abort == 0) break;
+      ensure_arena(end.abort_need);
+      reset_abort = true;
+      if (end.abort == kAbortAggArena) {
         // redo this level's aggregation with the host in charge, then continue captured
         if (!aggregate(-1)) break;
       }
+      prev = seg_counts();
       if (launch > 64) throw Fail{LV_ERR_DEVICE_CHECK, "captured run kept stopping for arena growth"};
     }
     finished = true;
@@ -996,7 +1093,7 @@ void lv_config_default(lv_config* c) {
   c->chunk_edges = 50000000;        // STEP_ROUND
   c->weight_mode = LV_WEIGHTS_AUTO;
   c->validate = 1;
-  c->use_graphs = 0;
+  c->use_graphs = 1;
 }
 
 lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
@@ -1016,6 +1113,7 @@ lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->pinned, 64);
+  if (e == cudaSuccess) e = ctx->slot.create();
   for (auto& ev : ctx->ev)
     if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) {
@@ -1030,6 +1128,7 @@ lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
 lv_status lv_destroy(lv_context* ctx) {
   if (!ctx) return LV_ERR_ARGUMENT;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->slot.destroy();
   ctx->drain_pool();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->ev)
@@ -1067,6 +1166,7 @@ lv_status lv_optimization_step(lv_community* c, double* delta_q, int64_t* n_move
   std::lock_guard<std::mutex> lk(c->ctx->mu);
   return guarded(c->ctx, [&] {
     lv::Run& r = *c->run;
+    r.bind();
     if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished (aggregation without contraction)"};
     lv::GraphState before;
     LV_CUDA(cudaMemcpy(&before, r.D.gs, sizeof(before), cudaMemcpyDeviceToHost));
@@ -1087,6 +1187,7 @@ lv_status lv_optimization_run(lv_community* c, int32_t* iterations) {
   std::lock_guard<std::mutex> lk(c->ctx->mu);
   return guarded(c->ctx, [&] {
     lv::Run& r = *c->run;
+    r.bind();
     if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
     r.force_iterating();
     const int32_t it = r.optimization_run();
@@ -1099,6 +1200,7 @@ lv_status lv_aggregation_run(lv_community* c, int32_t aggregate) {
   std::lock_guard<std::mutex> lk(c->ctx->mu);
   return guarded(c->ctx, [&] {
     lv::Run& r = *c->run;
+    r.bind();
     if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
     // the reference aggregates right after its optimisation loop; a graph still marked
     // iterating (phase-level callers) takes part as if its level had stopped
@@ -1113,6 +1215,7 @@ lv_status lv_louvain(lv_community* c, lv_stats* stats) {
   std::lock_guard<std::mutex> lk(c->ctx->mu);
   return guarded(c->ctx, [&] {
     lv::Run& r = *c->run;
+    r.bind();
     if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
     r.louvain();
     if (stats) r.stats(stats);
@@ -1169,6 +1272,7 @@ lv_status lv_community_get_graph(lv_community* c, int64_t* row_ptr, int32_t* col
   std::lock_guard<std::mutex> lk(c->ctx->mu);
   return guarded(c->ctx, [&] {
     lv::Run& r = *c->run;
+    r.bind();
     if (r.finished) throw Fail{LV_ERR_STATE, "the run has finished"};
     std::vector<uint32_t> hr(r.n + 1), hc(r.E), hw(r.E);
     std::vector<double> hk(r.n);

@@ -56,7 +56,14 @@ struct Dev {
   uint32_t* best;            // [n0] current-level vertex of each input vertex
   uint32_t* gid0;            // [n0] graph of each input vertex (nullptr: one graph)
   int32_t* out;              // [n0] final community ids
+  unsigned long long* scan_tmp;  // [(n + 1) / kScanTile + 2] tile sums of the scans
 };
+
+// The Dev of every live slot (a context's, each serving slot's), in constant memory: kernels
+// take the slot index and read their pointers through the constant cache, as fast as kernel
+// parameters, while a captured graph's arguments stay fixed from run to run.
+constexpr int kMaxDevSlots = 96;
+__constant__ Dev c_dev[kMaxDevSlots];
 
 struct BinCfg {
   uint32_t maxdeg[kNumBins];  // bin b: maxdeg[b-1] < d <= maxdeg[b]; the last bin is open
@@ -115,7 +122,8 @@ __device__ __forceinline__ bool has_nonloop(const Dev& D, uint32_t v, uint32_t d
 // phaseOptimizationSort.cu:46-86 / 186-240 walk the edges in chunks of STEP_ROUND and
 // `return` from the whole pass at the first chunk whose copy_if selects nothing; vertices
 // of that chunk and of every later chunk are not considered in that pass.
-__global__ void k_chunk_flags(Dev D) {
+__global__ void k_chunk_flags(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   if (blockIdx.x == 0 && threadIdx.x == 0) C->t_pass0 = global_ns();  // first kernel of a pass
   if (!C->chunk_on || !(C->fast || C->rule_sort)) return;
@@ -131,7 +139,8 @@ __global__ void k_chunk_flags(Dev D) {
 }
 
 // ---- pass: degree binning of the active vertices ----------------------------------------------
-__global__ void k_bin_vertices(Dev D, BinCfg B) {
+__global__ void k_bin_vertices(int dslot, BinCfg B) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n, it = C->it;
   uint32_t v_end = n;
@@ -377,7 +386,8 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 // they enter the argmax (the reference's own-community and negative candidates can never
 // win a move).
 template <int T, bool WINT>
-__global__ void __launch_bounds__(256) k_opt_team(Dev D, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(256) k_opt_team(int dslot, int bin, uint32_t cap) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -473,7 +483,8 @@ __device__ __forceinline__ unsigned long long block_max(unsigned long long x, un
 // a slice of the global arena at hub_off[idx] (vertices whose 2x degree exceeds shared
 // memory), touched through L2 atomics.
 template <bool WINT, bool GTABLE>
-__global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t cap) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -534,7 +545,8 @@ __global__ void __launch_bounds__(512) k_opt_block(Dev D, int bin, uint32_t cap)
 // long_items); pieces are scanned by separate blocks into the vertex's global table, the table is
 // evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
 // atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
-__global__ void k_opt_hub_prep(Dev D) {
+__global__ void k_opt_hub_prep(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[kNumBins - 1];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -553,7 +565,8 @@ __global__ void k_opt_hub_prep(Dev D) {
 }
 
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_opt_hub_scan(Dev D) {
+__global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   __shared__ unsigned long long red[33];
@@ -594,7 +607,8 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(Dev D) {
 }
 
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_opt_hub_eval(Dev D) {
+__global__ void __launch_bounds__(256) k_opt_hub_eval(int dslot) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   __shared__ unsigned long long red[33];
@@ -618,7 +632,8 @@ __global__ void __launch_bounds__(256) k_opt_hub_eval(Dev D) {
   }
 }
 
-__global__ void k_opt_hub_decide(Dev D) {
+__global__ void k_opt_hub_decide(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[kNumBins - 1], it = C->it;
   const bool fast = C->fast != 0;
@@ -683,7 +698,8 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
 
 // One warp per mover found by the team kernels.
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_apply(Dev D) {
+__global__ void __launch_bounds__(256) k_apply(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   // the optimisation kernels of this pass ended when the first apply block starts
   if (blockIdx.x == 0 && threadIdx.x == 0) C->t_optk_ns += global_ns() - C->t_pass0;
@@ -716,7 +732,8 @@ __global__ void __launch_bounds__(256) k_apply(Dev D) {
 // Movers found by the block kernels (vertices with long rows): one block per piece of
 // kHubPiece entries of their rows; the first piece also moves the totals.
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_apply_hub(Dev D) {
+__global__ void __launch_bounds__(512) k_apply_hub(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->apply_items, it = C->it;
   __shared__ long long shi[32];
@@ -756,7 +773,8 @@ __global__ void __launch_bounds__(512) k_apply_hub(Dev D) {
 // Integer mode squares exactly in u64 (a_c <= 2m < 2^32). One graph: per-block partials,
 // summed in a fixed order by k_finalize. Several graphs: one block per graph.
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_commit_sq(Dev D, int single) {
+__global__ void __launch_bounds__(256) k_commit_sq(int dslot, int single) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->mover_count, hubs = C->hub_mover_count, nn = C->n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count + hubs; i += gridDim.x * blockDim.x) {
@@ -835,8 +853,9 @@ __global__ void k_set_pass(Ctrl* C, uint32_t p, int mode, int fast_first) {
 // dQ <= threshold (or after EARLY_STOP_LIMIT passes). `level_start` = 1 evaluates the level's
 // starting modularity instead (Community::update -> compute_modularity, community.h:57-65).
 template <bool WINT>
-__global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts, int level_start,
+__global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int nparts, int level_start,
                                                    int mode, int fast_first, GraphCtl gc) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   __shared__ double shd[33];
   __shared__ unsigned long long shu[33];
@@ -927,7 +946,8 @@ __global__ void __launch_bounds__(1024) k_finalize(Dev D, int single, int nparts
 // ---- level start ------------------------------------------------------------------------------------
 // Community::update (community.h:57-65): identity partition, totals = k, every vertex active
 // (phaseOptimization.cuh:52).
-__global__ void k_level_init(Dev D) {
+__global__ void k_level_init(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n, it = C->it;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
@@ -952,7 +972,8 @@ __global__ void k_level_init(Dev D) {
 
 // Chunk bounds of the reference's edge loop for the current level (single graph):
 // limit = round + STEP; limit = (limit >= E) ? E : neighboorhood_sum[edge_source[limit] - 1].
-__global__ void k_chunk_bounds(Dev D, unsigned long long step) {
+__global__ void k_chunk_bounds(int dslot, unsigned long long step) {
+  const Dev& D = c_dev[dslot];
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n, E = C->E;
@@ -1015,8 +1036,9 @@ __device__ __forceinline__ void prep_entries(const Dev& D, uint32_t v, long long
 }
 
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, const float* wf_in,
+__global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64, const float* wf_in,
                                               uint32_t n, unsigned long long E) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1081,7 +1103,8 @@ __global__ void __launch_bounds__(256) k_prep(Dev D, const long long* row64, con
 
 // Rows longer than kPrepLongRow entries, one block each.
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_prep_long(Dev D, const float* wf_in) {
+__global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   __shared__ unsigned long long shu[33];
   __shared__ double shd[33];
@@ -1117,7 +1140,8 @@ __global__ void __launch_bounds__(512) k_prep_long(Dev D, const float* wf_in) {
 
 // m = (sum of k) / 2 per graph; integer mode requires 2m < 2^32 (the reference's u32 sums).
 template <bool WINT>
-__global__ void k_prep_total(Dev D) {
+__global__ void k_prep_total(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
     GraphState* st = &D.gs[g];
@@ -1181,7 +1205,8 @@ __global__ void k_rebase_pieces(long long* row64, uint32_t* col, const long long
 
 // Hash-table arena needed by the global-table bin at this level: sum over vertices with
 // degree above the shared-memory bound of next_pow2(2 d).
-__global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap) {
+__global__ void k_arena_need(int dslot, uint32_t min_deg, uint32_t block_cap) {
+  const Dev& D = c_dev[dslot];
   unsigned long long* need = &D.ctrl->arena_need;
   const uint32_t n = D.ctrl->n;
   unsigned long long s = 0;
@@ -1201,13 +1226,15 @@ __global__ void k_arena_need(Dev D, uint32_t min_deg, uint32_t block_cap) {
 // reference tests a_c > 0 (CountNotZero); with every weight positive that is exactly "has a
 // member", which is what is marked here, so no rounding residue in a_c can create an empty
 // row. The low word counts only communities of graphs that continue to a new level.
-__global__ void k_agg_mark(Dev D) {
+__global__ void k_agg_mark(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t n = D.ctrl->n;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
     D.map[D.comm[v]] = 1ull;
 }
 
-__global__ void k_agg_flags(Dev D) {
+__global__ void k_agg_flags(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t n = D.ctrl->n;
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const uint32_t g = D.gid ? D.gid[c] : 0u;
@@ -1217,7 +1244,8 @@ __global__ void k_agg_flags(Dev D) {
 }
 
 // Per graph: n_of_best_communities, base of its final ids, next-level vertex range.
-__global__ void k_agg_meta(Dev D) {
+__global__ void k_agg_meta(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < C->G; g += gridDim.x * blockDim.x) {
@@ -1234,7 +1262,8 @@ __global__ void k_agg_meta(Dev D) {
 
 // community.h:48-55 update_best: best[v0] = new(comm[best[v0]]). Graphs that stop here get
 // their final ids (0..K-1 within the graph) written to `out`.
-__global__ void k_agg_best(Dev D) {
+__global__ void k_agg_best(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n0 = C->n0;
   for (uint32_t v0 = blockIdx.x * blockDim.x + threadIdx.x; v0 < n0; v0 += gridDim.x * blockDim.x) {
@@ -1255,7 +1284,8 @@ __global__ void k_agg_best(Dev D) {
 
 // Count members and degree sums of each new community (packed, one atomic per vertex); the
 // returned old value is the vertex's rank inside its community.
-__global__ void k_agg_count(Dev D) {
+__global__ void k_agg_count(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t n = D.ctrl->n;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const uint32_t g = D.gid ? D.gid[v] : 0u;
@@ -1268,7 +1298,8 @@ __global__ void k_agg_count(Dev D) {
   }
 }
 
-__global__ void k_agg_scatter(Dev D) {
+__global__ void k_agg_scatter(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t n = D.ctrl->n;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const uint32_t g = D.gid ? D.gid[v] : 0u;
@@ -1289,7 +1320,8 @@ __device__ __forceinline__ uint32_t contract_cap(uint32_t dsum, uint32_t ng, boo
 // Bin the new communities by their summed member degree (the contraction's work). Bin 7
 // communities (the largest) are contracted by many blocks at once into a global table whose
 // arena offset is recorded per community in hubtab (kEmpty for every other community).
-__global__ void k_agg_bin(Dev D, BinCfg B) {
+__global__ void k_agg_bin(int dslot, BinCfg B) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n2 = C->n_next;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n2; base += gridDim.x * blockDim.x) {
@@ -1321,7 +1353,8 @@ __global__ void k_agg_bin(Dev D, BinCfg B) {
 
 // Bin-7 set-up once the arena is large enough: owner of every table chunk, and zeroed
 // accumulators (row length, k') of each such community.
-__global__ void k_hub_owner(Dev D, int bin) {
+__global__ void k_hub_owner(int dslot, int bin) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
@@ -1344,7 +1377,8 @@ __global__ void k_hub_owner(Dev D, int bin) {
 // Bin-7 insert: one warp per member vertex, all members of all large communities at once,
 // into their communities' global tables (L2 atomics).
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_hub_insert(Dev D) {
+__global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -1416,7 +1450,8 @@ __global__ void __launch_bounds__(256) k_hub_insert(Dev D) {
 
 // Pieces of the long rows deferred by k_hub_insert, one block per piece.
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_hub_insert_long(Dev D) {
+__global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -1461,7 +1496,8 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(Dev D) {
 // Bin-7 emit: one block per table chunk; occupied slots are appended to the community's row
 // (positions claimed with one atomic per block), k' and the self-loop weight accumulated.
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_hub_emit(Dev D) {
+__global__ void __launch_bounds__(512) k_hub_emit(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t nchunks = min(D.ctrl->hub_cursor, D.ctrl->arena_slots) / kHubChunk;
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
@@ -1549,7 +1585,8 @@ __device__ __forceinline__ CommCtx load_comm(const Dev& D, uint32_t s) {
 // unique destinations are written to colB/wB at the community's degree-sum offset, the row
 // length to newdeg, k' = row sum to kB, the self-loop weight to the graph's next-level I.
 template <int T, bool WINT>
-__global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint32_t cap) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -1657,7 +1694,8 @@ __global__ void __launch_bounds__(256) k_contract_team(Dev D, int bin, uint32_t 
 
 // One block per new community of bin 6 (shared-memory table).
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint32_t cap) {
+  const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -1774,7 +1812,8 @@ __global__ void __launch_bounds__(512) k_contract_block(Dev D, int bin, uint32_t
 constexpr uint32_t kCompactChunk = 2048;
 
 template <bool WINT>
-__global__ void __launch_bounds__(256) k_agg_compact(Dev D) {
+__global__ void __launch_bounds__(256) k_agg_compact(int dslot) {
+  const Dev& D = c_dev[dslot];
   using Wt = typename WTraits<WINT>::W;
   __shared__ uint32_t rs[kCompactChunk + 2];
   __shared__ uint32_t r0_sh, nr_sh;
@@ -1817,7 +1856,8 @@ __global__ void __launch_bounds__(256) k_agg_compact(Dev D) {
   }
 }
 
-__global__ void k_agg_finish(Dev D) {
+__global__ void k_agg_finish(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n2 = C->n_next;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s <= n2; s += gridDim.x * blockDim.x)
@@ -1850,7 +1890,8 @@ __global__ void k_agg_finish(Dev D) {
 
 // Which graphs aggregate now and whether they continue: modularityAlgorithms.h:52
 // cont = Q_end - Q_level_start > threshold. force >= 0 overrides (phase-level API).
-__global__ void k_agg_decide(Dev D, int force, uint32_t max_levels) {
+__global__ void k_agg_decide(int dslot, int force, uint32_t max_levels) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->t_agg0 = global_ns();
@@ -1871,13 +1912,15 @@ __global__ void k_agg_decide(Dev D, int force, uint32_t max_levels) {
 
 // ---- device-sized clears and the gates of a captured run ----------------------------------------
 // Aggregation scratch cleared to the level's own sizes (read on the device).
-__global__ void k_agg_clear_map(Dev D) {
+__global__ void k_agg_clear_map(int dslot) {
+  const Dev& D = c_dev[dslot];
   const uint32_t n = D.ctrl->n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) D.map[i] = 0ull;
 }
 // Before the contraction: per-new-community counters and hub offsets, and the counters the
 // binning appends with (so that an aggregation can be run again from its start).
-__global__ void k_agg_clear_next(Dev D) {
+__global__ void k_agg_clear_next(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n2 = C->n_next;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n2; i += gridDim.x * blockDim.x) {
@@ -1892,7 +1935,8 @@ __global__ void k_agg_clear_next(Dev D) {
   }
 }
 // The global contraction tables of this aggregation: empty keys, zero values.
-__global__ void k_arena_clear(Dev D) {
+__global__ void k_arena_clear(int dslot) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t used = min(C->hub_cursor, C->arena_slots);
   unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
@@ -1902,7 +1946,8 @@ __global__ void k_arena_clear(Dev D) {
   }
 }
 // Level body entry: the pass loop runs while some graph iterates.
-__global__ void k_gate_pass(Dev D, GraphCtl gc) {
+__global__ void k_gate_pass(int dslot, GraphCtl gc) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   if (C->seg_aggs > kGuardLevels) atomicOr(&C->err, kErrLoop);
   const bool stop = (C->err & kErrLoop) != 0;
@@ -1910,7 +1955,8 @@ __global__ void k_gate_pass(Dev D, GraphCtl gc) {
   if (stop) set_cond(gc, gc.level, false);
 }
 // After the renumbering: contract (then-branch) when some graph continues, else the run ends.
-__global__ void k_gate_contract(Dev D, GraphCtl gc) {
+__global__ void k_gate_contract(int dslot, GraphCtl gc) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const bool more = C->n_next > 0;
   if (more) C->seg_contract += 1; else C->seg_final += 1;
@@ -1920,7 +1966,8 @@ __global__ void k_gate_contract(Dev D, GraphCtl gc) {
 }
 // After the contraction binning: its global tables must fit the arena; if not, the run stops
 // here (nothing of this aggregation is final yet) and the host grows the arena and redoes it.
-__global__ void k_gate_arena_agg(Dev D, GraphCtl gc) {
+__global__ void k_gate_arena_agg(int dslot, GraphCtl gc) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const bool ok = C->hub_cursor <= C->arena_slots;
   if (ok) {
@@ -1934,7 +1981,8 @@ __global__ void k_gate_arena_agg(Dev D, GraphCtl gc) {
 }
 // End of a level start: the next level's optimisation tables must fit the arena; if not, the
 // run stops with the level started and the host grows the arena and resumes.
-__global__ void k_gate_level(Dev D, GraphCtl gc) {
+__global__ void k_gate_level(int dslot, GraphCtl gc) {
+  const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const bool ok = C->arena_need <= C->arena_slots;
   if (!ok) {
@@ -1945,35 +1993,62 @@ __global__ void k_gate_level(Dev D, GraphCtl gc) {
 }
 
 // ---- scans (3-phase: tile sums, scan of tile sums, tile scan + offset) ---------------------------
+// The three scans of an aggregation, each named by what it scans so that its arrays and length
+// come from the device state (a captured run replays them at every level with every size):
+//   kScanMap: map -> map, inclusive, n entries (community renumbering)
+//   kScanCd:  cd -> cd, exclusive, n_next + 1 entries (members and degree sums per community)
+//   kScanDeg: newdeg -> rowB, exclusive, n_next + 1 entries (next-level row offsets)
+// The blocks stride over tiles, so the grid does not depend on the size either.
 constexpr int kScanNT = 256;
 constexpr int kScanIPT = 8;
 constexpr int kScanTile = kScanNT * kScanIPT;
+enum : int { kScanMap = 0, kScanCd = 1, kScanDeg = 2 };
 
-// Every scan takes its length either from the host (dn == nullptr) or from the device
-// (*dn + add, read when the kernel runs), so a captured sequence scans each level's size.
-template <class T>
-__global__ void __launch_bounds__(kScanNT) k_scan_tiles(const T* in, T* tile_sums, uint32_t n,
-                                                        const uint32_t* dn, uint32_t add) {
-  __shared__ T sh[33];
-  if (dn) n = *dn + add;
-  if ((uint64_t)blockIdx.x * kScanTile >= n) return;
-  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
-  T s = T(0);
-#pragma unroll
-  for (int i = 0; i < kScanIPT; ++i) {
-    const uint64_t j = base + (uint64_t)i * kScanNT + threadIdx.x;
-    if (j < n) s += in[j];
-  }
-  T tot;
-  block_excl_scan<T, kScanNT>(s, sh, &tot);
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+template <int SRC>
+__device__ __forceinline__ uint32_t scan_len(const Dev& D) {
+  return SRC == kScanMap ? D.ctrl->n : D.ctrl->n_next + 1u;
+}
+template <class T, int SRC>
+__device__ __forceinline__ const T* scan_in(const Dev& D) {
+  if constexpr (SRC == kScanMap) return reinterpret_cast<const T*>(D.map);
+  else if constexpr (SRC == kScanCd) return reinterpret_cast<const T*>(D.cd);
+  else return reinterpret_cast<const T*>(D.newdeg);
+}
+template <class T, int SRC>
+__device__ __forceinline__ T* scan_out(const Dev& D) {
+  if constexpr (SRC == kScanMap) return reinterpret_cast<T*>(D.map);
+  else if constexpr (SRC == kScanCd) return reinterpret_cast<T*>(D.cd);
+  else return reinterpret_cast<T*>(D.rowB);
 }
 
-template <class T>
-__global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntiles,
-                                                    const uint32_t* dn, uint32_t add) {
+template <class T, int SRC>
+__global__ void __launch_bounds__(kScanNT) k_scan_tiles(int dslot) {
+  const Dev& D = c_dev[dslot];
   __shared__ T sh[33];
-  if (dn) ntiles = (*dn + add + kScanTile - 1) / kScanTile;
+  const uint32_t n = scan_len<SRC>(D);
+  const uint32_t ntiles = (n + kScanTile - 1) / kScanTile;
+  const T* in = scan_in<T, SRC>(D);
+  T* tile_sums = reinterpret_cast<T*>(D.scan_tmp);
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t base = (uint64_t)t * kScanTile;
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < kScanIPT; ++i) {
+      const uint64_t j = base + (uint64_t)i * kScanNT + threadIdx.x;
+      if (j < n) s += in[j];
+    }
+    T tot;
+    block_excl_scan<T, kScanNT>(s, sh, &tot);
+    if (threadIdx.x == 0) tile_sums[t] = tot;
+  }
+}
+
+template <class T, int SRC>
+__global__ void __launch_bounds__(1024) k_scan_sums(int dslot) {
+  const Dev& D = c_dev[dslot];
+  __shared__ T sh[33];
+  const uint32_t ntiles = (scan_len<SRC>(D) + kScanTile - 1) / kScanTile;
+  T* tile_sums = reinterpret_cast<T*>(D.scan_tmp);
   // each thread scans a contiguous run, then the block scans the run totals
   const uint32_t per = (ntiles + 1023) / 1024;
   const uint32_t b = threadIdx.x * per, e = min(b + per, ntiles);
@@ -1988,31 +2063,36 @@ __global__ void __launch_bounds__(1024) k_scan_sums(T* tile_sums, uint32_t ntile
   }
 }
 
-// inclusive = true: out[i] = sum in[0..i]; false: out[i] = sum in[0..i-1], and if
-// total_out != nullptr the grand total is written there.
-template <class T, bool INCLUSIVE>
-__global__ void __launch_bounds__(kScanNT) k_scan_apply(const T* in, T* out, const T* tile_offs,
-                                                         uint32_t n, const uint32_t* dn, uint32_t add) {
+// inclusive: out[i] = sum in[0..i]; exclusive: out[i] = sum in[0..i-1]. In place is fine: a
+// thread reads its own elements before it writes them.
+template <class T, int SRC, bool INCLUSIVE>
+__global__ void __launch_bounds__(kScanNT) k_scan_apply(int dslot) {
+  const Dev& D = c_dev[dslot];
   __shared__ T sh[33];
-  if (dn) n = *dn + add;
-  if ((uint64_t)blockIdx.x * kScanTile >= n) return;
-  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanIPT;
-  T vals[kScanIPT];
-  T s = T(0);
+  const uint32_t n = scan_len<SRC>(D);
+  const uint32_t ntiles = (n + kScanTile - 1) / kScanTile;
+  const T* in = scan_in<T, SRC>(D);
+  T* out = scan_out<T, SRC>(D);
+  const T* tile_offs = reinterpret_cast<const T*>(D.scan_tmp);
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t base = (uint64_t)t * kScanTile + (uint64_t)threadIdx.x * kScanIPT;
+    T vals[kScanIPT];
+    T s = T(0);
 #pragma unroll
-  for (int i = 0; i < kScanIPT; ++i) {
-    const uint64_t j = base + i;
-    vals[i] = j < n ? in[j] : T(0);
-    s += vals[i];
-  }
-  T tot;
-  T run = block_excl_scan<T, kScanNT>(s, sh, &tot) + tile_offs[blockIdx.x];
+    for (int i = 0; i < kScanIPT; ++i) {
+      const uint64_t j = base + i;
+      vals[i] = j < n ? in[j] : T(0);
+      s += vals[i];
+    }
+    T tot;
+    T run = block_excl_scan<T, kScanNT>(s, sh, &tot) + tile_offs[t];
 #pragma unroll
-  for (int i = 0; i < kScanIPT; ++i) {
-    const uint64_t j = base + i;
-    if (INCLUSIVE) run += vals[i];
-    if (j < n) out[j] = run;
-    if (!INCLUSIVE) run += vals[i];
+    for (int i = 0; i < kScanIPT; ++i) {
+      const uint64_t j = base + i;
+      if (INCLUSIVE) run += vals[i];
+      if (j < n) out[j] = run;
+      if (!INCLUSIVE) run += vals[i];
+    }
   }
 }
 

@@ -62,6 +62,7 @@ struct lv_server {
   std::vector<std::thread> workers;
   std::vector<cudaStream_t> streams;
   std::vector<uint32_t*> pinned;  // per slot: 64-byte readback buffer
+  std::vector<std::unique_ptr<lv::DevSlot>> dslots;  // per slot: Dev buffer and captured graph
 
   // Continuous batching: a free slot takes the request at the head of the queue and, when
   // that request is small, every further queued request (in arrival order) that is small too,
@@ -136,7 +137,7 @@ struct lv_server {
 
   void run_batch(const std::vector<lv::Request*>& batch, int slot) {
     try {
-      lv::Run run(ctx, streams[slot], pinned[slot]);
+      lv::Run run(ctx, streams[slot], pinned[slot], dslots[slot].get());
       std::vector<lv::Run::Piece> ps;
       ps.reserve(batch.size());
       for (lv::Request* r : batch) {
@@ -179,7 +180,7 @@ struct lv_server {
 extern "C" {
 
 lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_slots, lv_server** out) {
-  if (!ctx || !out || budget_bytes <= 0 || max_slots <= 0 || max_slots > 256) return LV_ERR_ARGUMENT;
+  if (!ctx || !out || budget_bytes <= 0 || max_slots <= 0 || max_slots > 64) return LV_ERR_ARGUMENT;
   *out = nullptr;
   auto s = std::make_unique<lv_server>();
   s->ctx = ctx;
@@ -202,6 +203,15 @@ lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_sl
       return LV_ERR_CUDA;
     }
     s->pinned.push_back(pb);
+    auto ds = std::make_unique<lv::DevSlot>();
+    if (ds->create() != cudaSuccess) {
+      for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+      for (uint32_t* x : s->pinned) cudaFreeHost(x);
+      for (auto& d : s->dslots) d->destroy();
+      cudaGetLastError();
+      return LV_ERR_CUDA;
+    }
+    s->dslots.push_back(std::move(ds));
   }
   lv_server* p = s.get();
   for (int i = 0; i < max_slots; ++i) s->workers.emplace_back([p, i] { p->worker(i); });
@@ -226,6 +236,7 @@ lv_status lv_server_destroy(lv_server* s) {
   for (auto& t : s->workers) t.join();
   for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
   for (uint32_t* pb : s->pinned) cudaFreeHost(pb);
+  for (auto& d : s->dslots) d->destroy();
   delete s;
   return LV_OK;
 }

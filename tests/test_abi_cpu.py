@@ -74,6 +74,10 @@ def test_config_defaults_follow_reference_constants(lv):
     assert c.chunk_edges == 50_000_000   # constants.h:18
     assert c.max_iterations == 1_000_000_000  # constants.h:16
     assert c.fast_first == 1
+    # the library's own default (lv_config_default), not only the Python wrapper's
+    raw = lv.Config()
+    lv.load_library().lv_config_default(raw)
+    assert raw.use_graphs == 1 and raw.validate == 1 and raw.weight_mode == lv.WEIGHTS_AUTO
 
 
 def test_status_strings(lv):
