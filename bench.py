@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--pool", type=int, default=64, help="served: distinct request graphs")
     ap.add_argument("--slots", type=int, default=16, help="served: concurrent server slots")
     ap.add_argument("--rates", default="10,50,200,1000,2000", help="served: arrival rates, req/s")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in degree-bin table (default: tune on a sample first)")
     ap.add_argument("--captured", type=int, default=-1, choices=[-1, 0, 1],
                     help="1: run the level loop as one captured CUDA graph, 0: host-driven, "
                          "-1: the library default")
@@ -246,6 +248,21 @@ def run_batched(args, local):
     eng = lv.Engine(local, mode=mode, use_graphs=True)
     plain = lv.Engine(local, mode=mode)
     N = int(b.n.sum())
+    # autotune the batch engine's degree bins on a sample: every 16th graph, packed
+    tune = {}
+    if not args.no_autotune:
+        idx = list(range(0, b.G, 16))
+        sub = [b.graph(g) for g in idx]
+        offs_s = np.zeros(len(sub) + 1, dtype=np.int64)
+        offs_s[1:] = np.cumsum([n for n, _, _ in sub])
+        eoffs = np.zeros(len(sub) + 1, dtype=np.int64)
+        eoffs[1:] = np.cumsum([int(rp[-1]) for _, rp, _ in sub])
+        row_s = torch.cat([sub[0][1][:1]] + [rp[1:] + int(eoffs[i]) for i, (_, rp, _) in enumerate(sub)])
+        col_s = torch.cat([cl + int(offs_s[i]) for i, (_, _, cl) in enumerate(sub)]).to(torch.int32)
+        t0 = time.perf_counter()
+        bins, tms = eng.autotune(torch.from_numpy(offs_s).to(dev), row_s, col_s, trials=2)
+        tune = {"sample": f"every 16th graph ({len(sub)} graphs)", "bins": bins[:7],
+                "best_sample_ms": tms, "tuning_s": time.perf_counter() - t0}
     out_d = torch.empty(N, dtype=torch.int32, device=dev)
     for _ in range(max(1, args.warmup)):
         eng.run_batch(b.vtx_offsets, b.row_ptr, b.col, out=out_d)
@@ -293,6 +310,7 @@ def run_batched(args, local):
         "clocks": clk.summary(),
     }
     line["graph_launches"] = int(st.graph_launches)
+    line["autotune"] = tune
     print(json.dumps(line), flush=True)
     eng.close()
     plain.close()
@@ -329,6 +347,16 @@ def run_served(args, local):
     torch.cuda.empty_cache()
     kw = {} if args.captured < 0 else {"use_graphs": bool(args.captured)}
     eng = lv.Engine(local, **kw)
+    tune = {}
+    if not args.no_autotune:
+        import importlib as _il
+        batch = _il.import_module(PKG + ".batch")
+        sample = pool[::8]
+        offs_s, row_s, col_s, _ = batch.pack(sample)
+        t0 = time.perf_counter()
+        bins, tms = eng.autotune(offs_s, row_s, col_s, trials=2)
+        tune = {"sample": f"every 8th pool graph ({len(sample)} graphs)", "bins": bins[:7],
+                "best_sample_ms": tms, "tuning_s": time.perf_counter() - t0}
     # loop baseline: the pool once, one call per request, host buffers in and out
     for g in pool[:4]:
         eng.run_graph(g)
@@ -386,6 +414,7 @@ def run_served(args, local):
         "speedup_vs_loop": best["graphs_per_s"] / loop_gps,
         "parity": {"max_abs_dq_vs_alone": worst_dq},
         "clocks": clk.summary(),
+        "autotune": tune,
     }
     print(json.dumps(line), flush=True)
     srv.close()
@@ -416,6 +445,15 @@ def main():
     mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
     kw = {} if args.captured < 0 else {"use_graphs": bool(args.captured)}
     eng = lv.Engine(local, mode=mode, **kw)
+    tune = {}
+    if not args.no_autotune and not args.once:
+        # tuned on a smaller graph of the same generator (scale - 2), never on the timed graph
+        gs = build_graph(max(10, args.scale - 2), device=dev)
+        t0 = time.perf_counter()
+        bins, tms = eng.autotune(np.array([0, gs.n], dtype=np.int64), gs.row_ptr, gs.col, trials=2)
+        tune = {"sample": f"R-MAT scale {max(10, args.scale - 2)} ef16 (n={gs.n})", "bins": bins[:7],
+                "best_sample_ms": tms, "tuning_s": time.perf_counter() - t0}
+        del gs
 
     row_d = torch.from_numpy(g.row_ptr).to(dev)
     col_d = torch.from_numpy(g.col).to(dev)
@@ -498,6 +536,7 @@ def main():
                      "peak_source": peak_kind},
         "clocks": clk.summary(),
         "gpu_launches": int(sum(s.kernel_launches for s in stats)),
+        "autotune": tune,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args)

@@ -146,6 +146,17 @@ lv_status lv_run_batch(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_off
                        int32_t in_mem, int32_t* out_comm, int32_t out_mem,
                        double* out_modularity, int32_t* out_ncomm, lv_stats* stats);
 
+/* Autotuner (no reference counterpart): times full runs of a sample -- one graph
+ * (n_graphs = 1, vtx_offsets = {0, n}) or a packed batch -- under a fixed set of candidate
+ * degree-bin tables (the boundaries that pick 4 / 8 / 16 / 32 lanes, a block or many blocks
+ * per row, and with them each row's hash-table capacity), `trials` runs each, keeps the
+ * fastest. The chosen table becomes the context's cfg.bin_max_degree for later runs and is
+ * returned in *out_cfg; *out_ms = its best run time. Results do not depend on the table for
+ * integer weights (every table computes the same sums). */
+lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offsets,
+                      const int64_t* row_ptr, const int32_t* col, const float* w, int32_t in_mem,
+                      int32_t trials, lv_config* out_cfg, double* out_ms);
+
 /* ---- phase-level interface ----------------------------------------------------------------
  * The reference's own phase boundaries, so callers (and parity tests) can step a run pass
  * by pass the way modularity_routine does. */

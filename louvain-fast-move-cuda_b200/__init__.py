@@ -97,7 +97,7 @@ TRACE_DTYPE = np.dtype([
 # Every entry point the header declares; tests check that the library exports all of them.
 EXPORTS = (
     "lv_config_default", "lv_create", "lv_destroy", "lv_last_error", "lv_status_string",
-    "lv_abi_version", "lv_run_csr", "lv_run_batch", "lv_community_create",
+    "lv_abi_version", "lv_run_csr", "lv_run_batch", "lv_autotune", "lv_community_create",
     "lv_community_destroy", "lv_optimization_step", "lv_optimization_run",
     "lv_aggregation_run", "lv_louvain", "lv_community_info_get", "lv_community_get_partition",
     "lv_community_get_best", "lv_community_get_graph", "lv_community_get_trace",
@@ -127,6 +127,7 @@ def load_library(path: Optional[str] = None):
         "lv_abi_version": (i32, []),
         "lv_run_csr": (i32, [vp, i64, vp, vp, vp, i32, vp, i32, P(dbl), P(Stats)]),
         "lv_run_batch": (i32, [vp, i32, vp, vp, vp, vp, i32, vp, i32, vp, vp, P(Stats)]),
+        "lv_autotune": (i32, [vp, i32, vp, vp, vp, vp, i32, i32, P(Config), P(dbl)]),
         "lv_community_create": (i32, [vp, i64, vp, vp, vp, i32, P(vp)]),
         "lv_community_destroy": (i32, [vp]),
         "lv_optimization_step": (i32, [vp, P(dbl), P(i64)]),
@@ -265,6 +266,26 @@ class Engine:
                                   qs.ctypes.data, ks.ctypes.data, ctypes.byref(s))
         self.check(st, "lv_run_batch")
         return out, qs, ks, s
+
+    def autotune(self, vtx_offsets, row_ptr, col, w=None, trials: int = 2):
+        """lv_autotune on a sample (a packed batch, or one graph with vtx_offsets = [0, n]):
+        installs the fastest degree-bin table in this engine. Returns (bins[8], best_ms)."""
+        dev = _is_device(row_ptr)
+        if not dev:
+            vtx_offsets = np.ascontiguousarray(vtx_offsets, dtype=np.int64)
+            row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+            G = vtx_offsets.size - 1
+        else:
+            G = int(vtx_offsets.numel()) - 1
+        out = Config()
+        ms = ctypes.c_double(0)
+        self.check(self._L.lv_autotune(self._h, G, _ptr(vtx_offsets), _ptr(row_ptr), _ptr(col), _ptr(w),
+                                       MEM_DEVICE if dev else MEM_HOST, int(trials), ctypes.byref(out),
+                                       ctypes.byref(ms)), "lv_autotune")
+        self.cfg = out
+        return list(out.bin_max_degree), ms.value
 
     def community(self, g: CSRGraph) -> "CommunityState":
         return CommunityState(self, g)

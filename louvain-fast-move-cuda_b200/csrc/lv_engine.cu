@@ -151,8 +151,19 @@ struct Fail {
   } while (0)
 
 // Default degree bins: team sizes 4/8/16/32 lanes with tables of 2x the bin's maximum
-// degree, a block per vertex up to 8192 entries (16K-slot shared table), global tables above.
-static const uint32_t kDefaultMaxDeg[kNumBins] = {4, 8, 16, 32, 128, 512, 8192, 0xFFFFFFFFu};
+// degree, a block per vertex up to 4096 entries (8K-slot shared table, several blocks per SM),
+// multi-block global tables above. lv_autotune replaces the table per workload.
+static const uint32_t kDefaultMaxDeg[kNumBins] = {4, 8, 16, 32, 128, 512, 4096, 0xFFFFFFFFu};
+
+// The autotuner's candidate tables (bins 0-6; bin 7 is open). Each moves the boundaries that
+// decide how many lanes serve a row (4 / 8 / 16 / 32 / 32 / 32 / a block / many blocks) and so
+// the table capacity each row gets (2x its bin's maximum degree, rounded to a power of two).
+static const int32_t kTuneCandidates[][7] = {
+    {4, 8, 16, 32, 128, 512, 4096},  {4, 8, 16, 32, 128, 512, 8192},  {4, 8, 16, 32, 128, 512, 2048},
+    {8, 16, 32, 64, 128, 512, 4096}, {2, 4, 8, 16, 64, 512, 4096},    {4, 8, 16, 32, 64, 256, 4096},
+    {4, 8, 16, 32, 128, 1024, 4096}, {8, 16, 32, 64, 256, 1024, 4096}, {8, 16, 32, 64, 128, 512, 2048},
+};
+constexpr int kTuneN = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
 static const int kTeamT[6] = {4, 8, 16, 32, 32, 32};
 
 struct Block {
@@ -1361,6 +1372,50 @@ lv_status lv_run_csr(lv_context* ctx, int64_t n, const int64_t* row_ptr, const i
                      double* out_modularity, lv_stats* stats) {
   return run_common(ctx, 1, nullptr, n, row_ptr, col, w, in_mem, out_comm, out_mem, out_modularity,
                     nullptr, stats);
+}
+
+lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offsets,
+                      const int64_t* row_ptr, const int32_t* col, const float* w, int32_t in_mem,
+                      int32_t trials, lv_config* out_cfg, double* out_ms) {
+  if (!ctx || n_graphs <= 0 || !vtx_offsets || !row_ptr || !col || trials <= 0 || trials > 16)
+    return LV_ERR_ARGUMENT;
+  using lv::kTuneCandidates;
+  using lv::kTuneN;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->device);
+    int64_t n = 0;  // vertices of the sample (vtx_offsets = {0, n} for one graph)
+    if (in_mem == LV_MEM_DEVICE) LV_CUDA(cudaMemcpy(&n, vtx_offsets + n_graphs, 8, cudaMemcpyDeviceToHost));
+    else n = vtx_offsets[n_graphs];
+    const lv_config base = ctx->cfg;
+    double best_ms = 1e300;
+    int best = -1;
+    for (int c = 0; c < kTuneN; ++c) {
+      double ms_c = 1e300;
+      for (int t = 0; t < trials; ++t) {
+        lv::Run r(ctx);
+        for (int b = 0; b < 7; ++b) r.cfg.bin_max_degree[b] = kTuneCandidates[c][b];
+        r.cfg.bin_max_degree[7] = 0;
+        LV_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        r.init((uint32_t)n_graphs, n_graphs > 1 ? vtx_offsets : nullptr, n, row_ptr, col, w, in_mem);
+        r.louvain();
+        LV_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        LV_CUDA(cudaEventSynchronize(ctx->ev[1]));
+        float ms = 0;
+        LV_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        ms_c = std::min(ms_c, (double)ms);
+      }
+      if (ms_c < best_ms) {
+        best_ms = ms_c;
+        best = c;
+      }
+    }
+    ctx->cfg = base;
+    for (int b = 0; b < 7; ++b) ctx->cfg.bin_max_degree[b] = kTuneCandidates[best][b];
+    ctx->cfg.bin_max_degree[7] = 0;
+    if (out_cfg) *out_cfg = ctx->cfg;
+    if (out_ms) *out_ms = best_ms;
+  });
 }
 
 lv_status lv_run_batch(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offsets,

@@ -102,6 +102,7 @@ def test_invalid_arguments_rejected_before_device_work(lv):
     assert L.lv_run_csr(None, 1, None, None, None, 0, None, 0, None, None) == 1
     assert L.lv_community_destroy(None) == 1
     assert L.lv_server_create(None, 1, 1, None) == 1
+    assert L.lv_autotune(None, 1, None, None, None, None, 0, 1, None, None) == 1
     f = L.lv_modularity_noalloc if hasattr(L, "lv_modularity_noalloc") else None
     if f is not None:
         f.restype = ctypes.c_int32
