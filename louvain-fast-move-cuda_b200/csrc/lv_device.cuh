@@ -103,6 +103,7 @@ struct Ctrl {
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
   uint32_t long_count;         // aggregation: pieces of long rows for k_hub_insert_long
+  uint32_t long_movers;        // pass: team-kernel movers with long rows, for k_apply_long
   uint32_t hub_items;          // pass: pieces of the bin-7 (global-table) vertices' rows
   uint32_t apply_items;        // pass: pieces of the rows of movers found by block kernels
   uint32_t hub_cursor;         // global hash-table arena cursor (slots)

@@ -636,10 +636,11 @@ class Run {
     k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(Dd);
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[5], st));
     k_apply<WI><<<grid_n, 256, 0, st>>>(Dd);
+    k_apply_long<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
     commit_sq();
     finalize(0);
-    launches += 17;
+    launches += 18;
   }
 
   // Runs one pass; returns the number of graphs still iterating.

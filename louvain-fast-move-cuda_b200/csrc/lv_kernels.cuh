@@ -696,10 +696,21 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
   }
 }
 
-// One warp per mover found by the team kernels.
+// Movers found by the team kernels, 32 per warp (one per lane): the warp walks the entries of
+// all 32 rows together -- lane i takes entries i, i+32, ... of the concatenated rows, kBatch at
+// a time -- so every lane is busy and keeps kBatch independent gathers in flight however short
+// the rows are (most movers have a handful of entries). Rows longer than kApplyShort are left
+// to k_apply_long (a warp each; movers sit in the list grouped by degree, so a warp taking 32
+// long rows would hold up the whole kernel). An entry's change of the internal weight goes to
+// its own graph, which is the mover's (edges never cross graphs).
+constexpr uint32_t kApplyShort = 32;
+
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_apply(int dslot) {
   const Dev& D = c_dev[dslot];
+  using Tr = WTraits<WINT>;
+  using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   Ctrl* C = D.ctrl;
   // the optimisation kernels of this pass ended when the first apply block starts
   if (blockIdx.x == 0 && threadIdx.x == 0) C->t_optk_ns += global_ns() - C->t_pass0;
@@ -707,15 +718,117 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t idx = warp; idx < count; idx += nwarps) {
-    const uint32_t v = D.movers[idx];
-    const uint32_t old = D.comm[v], nw = D.new_comm[v];
-    const double kv = D.k[v];
-    const uint32_t g = D.gid ? D.gid[v] : 0u;
-    if (lane == 0) {
+  uint32_t gcur = 0;  // graph of the running internal-weight change
+  long long di = 0;
+  double df = 0.0;
+  auto flush = [&]() {
+    if (WINT) {
+      if (di) atomicAdd(&D.gs[gcur].I, (unsigned long long)di);
+    } else if (df != 0.0) {
+      atomicAdd(reinterpret_cast<double*>(&D.gs[gcur].I), df);
+    }
+    di = 0;
+    df = 0.0;
+  };
+  for (uint32_t base = warp * 32u; base < count; base += nwarps * 32u) {
+    const uint32_t idx = base + lane;
+    uint32_t rs = 0, len = 0, old = 0, nw = 0, v = 0;
+    if (idx < count) {
+      v = D.movers[idx];
+      old = D.comm[v];
+      nw = D.new_comm[v];
+      rs = D.row[v];
+      len = D.row[v + 1] - rs;
+      const double kv = D.k[v];
       atomicAdd(&D.a[nw], kv);
       atomicAdd(&D.a[old], -kv);
     }
+    // long rows: queued for k_apply_long (the list lives in `members`, unused during passes)
+    const bool defer = len > kApplyShort;
+    const unsigned dm = __ballot_sync(kFull, defer);
+    if (dm) {
+      uint32_t b0 = 0;
+      if (lane == __ffs(dm) - 1) b0 = atomicAdd(&C->long_movers, (uint32_t)__popc(dm));
+      b0 = __shfl_sync(kFull, b0, __ffs(dm) - 1);
+      if (defer) D.members[b0 + __popc(dm & lanemask_lt())] = v;
+    }
+    if (defer) len = 0;
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t excl = incl - len;
+    for (uint32_t jb = 0; jb < total; jb += 32u * kBatch) {
+      uint32_t ee[kBatch], oo[kBatch], nn[kBatch], uu[kBatch], pre[kBatch], mv[kBatch];
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        const uint32_t j = jb + (uint32_t)q * 32u + lane;
+        int k = 0;  // owner: the last lane whose row starts at or before j
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const uint32_t ex = __shfl_sync(kFull, excl, k + step);
+          if (ex <= j) k += step;
+        }
+        ee[q] = __shfl_sync(kFull, rs, k) + (j - __shfl_sync(kFull, excl, k));
+        oo[q] = __shfl_sync(kFull, old, k);
+        nn[q] = __shfl_sync(kFull, nw, k);
+        uu[q] = j < total ? D.col[ee[q]] : kEmpty;
+      }
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        pre[q] = uu[q] != kEmpty ? D.comm[uu[q]] : 0u;
+        mv[q] = uu[q] != kEmpty ? D.moved_it[uu[q]] : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        if (uu[q] == kEmpty) continue;
+        const uint32_t u = uu[q];
+        const bool mu = mv[q] == it;
+        const uint32_t post = mu ? D.new_comm[u] : pre[q];
+        if (post != nn[q]) D.active_it[u] = it + 1;
+        const int dd = (int)(nn[q] == post) - (int)(oo[q] == pre[q]);
+        if (dd) {
+          const int f = mu ? dd : 2 * dd;
+          if (D.gid) {
+            const uint32_t g = D.gid[u];
+            if (g != gcur) {
+              flush();
+              gcur = g;
+            }
+          }
+          if (WINT) di += (long long)f * (long long)w[ee[q]];
+          else df += (double)f * Tr::w_double(w[ee[q]]);
+        }
+      }
+    }
+  }
+  if (!D.gid) {
+    // one graph: a single sum per warp
+    di = warp_sum(di);
+    df = warp_sum(df);
+    if (lane == 0) flush();
+  } else {
+    flush();
+  }
+}
+
+// The team kernels' movers with rows longer than kApplyShort (queued by k_apply, which also
+// moved their totals): one warp per mover, kBatch gathers in flight per lane.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_apply_long(int dslot) {
+  const Dev& D = c_dev[dslot];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->long_movers, it = C->it;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t idx = warp; idx < count; idx += nwarps) {
+    const uint32_t v = D.members[idx];
+    const uint32_t old = D.comm[v], nw = D.new_comm[v];
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
     long long di = 0;
     double df = 0.0;
     apply_entries<WINT>(D, v, old, nw, it, D.row[v] + lane, D.row[v + 1], 32, di, df);
@@ -918,6 +1031,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
     C->loop_continue = tot > 0;
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->mover_count = 0;
+    C->long_movers = 0;
     C->hub_mover_count = 0;
     C->hub_items = 0;
     C->apply_items = 0;
@@ -960,6 +1074,7 @@ __global__ void k_level_init(int dslot) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->mover_count = 0;
+    C->long_movers = 0;
     C->hub_mover_count = 0;
     C->hub_items = 0;
     C->apply_items = 0;
