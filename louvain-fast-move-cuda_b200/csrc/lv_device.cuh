@@ -268,6 +268,55 @@ __device__ __forceinline__ Acc table_get(const uint32_t* keys, const Acc* vals, 
   return Acc(0);
 }
 
+// Table views for the insert / scan loops. SplitTable: keys and sums in two arrays (shared-memory
+// tables, and global tables with fp32 weights). PackedTable: one u64 per slot, community id in
+// the high word and the integer weight sum in the low word (global tables with integer weights:
+// every sum is below 2m < 2^32, so adding to the low word never carries into the id); an
+// insert is one 64-bit atomic on one 8-byte slot instead of a CAS and an add on two arrays.
+constexpr unsigned long long kEmptySlot = 0xFFFFFFFF00000000ull;
+
+template <class Acc>
+struct SplitTable {
+  uint32_t* keys;
+  Acc* vals;
+  uint32_t mask, shift;
+  __device__ __forceinline__ bool add(uint32_t c, Acc w) const {
+    return table_add(keys, vals, mask, shift, c, w);
+  }
+  __device__ __forceinline__ void load(uint32_t i, uint32_t& k, Acc& v) const {
+    k = keys[i];
+    v = vals[i];
+  }
+};
+
+struct PackedTable {
+  unsigned long long* slots;
+  uint32_t mask, shift;
+  __device__ __forceinline__ bool add(uint32_t c, uint32_t w) const {
+    uint32_t h = hash_slot(c, shift);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      unsigned long long cur = ((volatile unsigned long long*)slots)[h];
+      uint32_t key = (uint32_t)(cur >> 32);
+      if (key == kEmpty) {
+        cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
+        if (cur == kEmptySlot) return true;
+        key = (uint32_t)(cur >> 32);
+      }
+      if (key == c) {
+        atomicAdd(&slots[h], (unsigned long long)w);
+        return true;
+      }
+      h = (h + 1) & mask;
+    }
+    return false;
+  }
+  __device__ __forceinline__ void load(uint32_t i, uint32_t& k, uint32_t& v) const {
+    const unsigned long long x = slots[i];
+    k = (uint32_t)(x >> 32);
+    v = (uint32_t)x;
+  }
+};
+
 // ---- warp / block reductions -------------------------------------------------------------------
 template <int T>
 __device__ __forceinline__ unsigned long long team_max(unsigned long long x, unsigned mask) {

@@ -630,7 +630,7 @@ class Run {
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
     k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
-    k_opt_hub_prep<<<ctx->sms * 4, 256, 0, st>>>(Dd);
+    k_opt_hub_prep<WI><<<ctx->sms * 4, 256, 0, st>>>(Dd);
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(Dd);
@@ -693,7 +693,7 @@ class Run {
   void agg_contract_b() {
     const size_t slot = 4 + (WI ? 4 : 8);
     // the largest new communities: many blocks insert into their global tables
-    k_arena_clear<<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    k_arena_clear<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(Dd, kNumBins - 1);
     k_hub_insert<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);

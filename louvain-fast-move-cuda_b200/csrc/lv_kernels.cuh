@@ -301,12 +301,10 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
 
 // Table pass, insert half: non-loop entries into the table by destination community, the
 // vertex's own community summed into self_acc.
-template <bool WINT>
+template <bool WINT, class Tbl>
 __device__ __forceinline__ void insert_scan(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t e0,
-                                            uint32_t step, uint32_t* keys,
-                                            typename WTraits<WINT>::Acc* vals, uint32_t mask,
-                                            uint32_t shift, typename WTraits<WINT>::Acc& self_acc,
-                                            uint32_t& err) {
+                                            uint32_t step, const Tbl& tbl,
+                                            typename WTraits<WINT>::Acc& self_acc, uint32_t& err) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
@@ -327,16 +325,14 @@ __device__ __forceinline__ void insert_scan(const Dev& D, const VtxCtx& x, uint3
     for (int k = 0; k < kBatch; ++k) {
       if (cc[k] == kEmpty) continue;
       if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
-      if (!table_add(keys, vals, mask, shift, cc[k], ww[k])) err |= kErrTableFull;
+      if (!tbl.add(cc[k], ww[k])) err |= kErrTableFull;
     }
   }
 }
 
 // Table pass, evaluation half: best key over the table's communities (slots s0, s0+step, ...).
-template <bool WINT>
-__device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxCtx& x,
-                                                        const uint32_t* keys,
-                                                        const typename WTraits<WINT>::Acc* vals,
+template <bool WINT, class Tbl>
+__device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxCtx& x, const Tbl& tbl,
                                                         uint32_t s0, uint32_t cap, uint32_t step,
                                                         float self_v, bool lowest) {
   using Tr = WTraits<WINT>;
@@ -350,9 +346,9 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       const uint32_t sk = s + k * step;
-      const bool in = sk < cap;
-      cc[k] = in ? keys[sk] : kEmpty;
-      vv[k] = in ? vals[sk] : Acc(0);
+      cc[k] = kEmpty;
+      vv[k] = Acc(0);
+      if (sk < cap) tbl.load(sk, cc[k], vv[k]);
       if (cc[k] == x.cv) cc[k] = kEmpty;
     }
 #pragma unroll
@@ -423,10 +419,11 @@ __global__ void __launch_bounds__(256) k_opt_team(int dslot, int bin, uint32_t c
       __syncwarp();
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
-      if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, keys, vals, mask, shift, self_acc, err);
+      const SplitTable<Acc> tbl{keys, vals, mask, shift};
+      if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, tbl, self_acc, err);
       self_acc = team_sum<T>(self_acc);
       __syncwarp();
-      if (live) best = cand_scan<WINT>(D, x, keys, vals, lane, cap_v, T, Tr::to_float(self_acc), lowest);
+      if (live) best = cand_scan<WINT>(D, x, tbl, lane, cap_v, T, Tr::to_float(self_acc), lowest);
       best = team_max<T>(best, kFull);
       __syncwarp();
     }
@@ -526,9 +523,10 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
         for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
       __syncthreads();
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
-      if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, keys, vals, mask, shift, self_acc, err);
+      const SplitTable<Acc> tbl{keys, vals, mask, shift};
+      if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, tbl, self_acc, err);
       self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
-      if (ok) best = cand_scan<WINT>(D, x, keys, vals, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
+      if (ok) best = cand_scan<WINT>(D, x, tbl, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
     }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best) {
@@ -545,6 +543,19 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
 // long_items); pieces are scanned by separate blocks into the vertex's global table, the table is
 // evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
 // atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
+// Global tables are packed (key << 32 | sum) with integer weights, split arrays with fp32 ones.
+template <bool WINT>
+__device__ __forceinline__ void arena_clear_slot(const Dev& D, uint32_t s) {
+  unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
+  if (WINT) {
+    vals[s] = kEmptySlot;
+  } else {
+    D.arena_keys[s] = kEmpty;
+    vals[s] = 0ull;
+  }
+}
+
+template <bool WINT>
 __global__ void k_opt_hub_prep(int dslot) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
@@ -556,11 +567,7 @@ __global__ void k_opt_hub_prep(int dslot) {
   }
   if (!C->fast) {
     const uint32_t slots = min(C->hub_cursor, C->arena_slots);
-    unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
-    for (uint32_t s = tid; s < slots; s += nth) {
-      D.arena_keys[s] = kEmpty;
-      vals[s] = 0ull;
-    }
+    for (uint32_t s = tid; s < slots; s += nth) arena_clear_slot<WINT>(D, s);
   }
 }
 
@@ -592,10 +599,17 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
       const bool ok = (unsigned long long)off + cap <= C->arena_slots;
       if (!ok) err |= kErrArena;
       Acc self_acc = Acc(0);
-      if (ok)
-        insert_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x, D.arena_keys + off,
-                          reinterpret_cast<Acc*>(D.arena_vals) + off, cap - 1u,
-                          32u - log2_pow2(cap), self_acc, err);
+      if (ok) {
+        if constexpr (WINT) {
+          const PackedTable tbl{reinterpret_cast<unsigned long long*>(D.arena_vals) + off, cap - 1u,
+                                32u - log2_pow2(cap)};
+          insert_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x, tbl, self_acc, err);
+        } else {
+          const SplitTable<Acc> tbl{D.arena_keys + off, reinterpret_cast<Acc*>(D.arena_vals) + off,
+                                    cap - 1u, 32u - log2_pow2(cap)};
+          insert_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x, tbl, self_acc, err);
+        }
+      }
       self_acc = block_sum<256>(self_acc, reinterpret_cast<Acc*>(red));
       if (threadIdx.x == 0 && self_acc != Acc(0)) {
         if (WINT) atomicAdd(&D.hubself[pos], (unsigned long long)self_acc);
@@ -625,8 +639,16 @@ __global__ void __launch_bounds__(256) k_opt_hub_eval(int dslot) {
     float self_v;
     if (WINT) self_v = Tr::to_float((Acc)hs);
     else self_v = Tr::to_float((Acc)__longlong_as_double((long long)hs));
-    unsigned long long best = cand_scan<WINT>(D, x, D.arena_keys, vals, c * kHubChunk + threadIdx.x,
-                                              (c + 1) * kHubChunk, blockDim.x, self_v, lowest);
+    unsigned long long best;
+    if constexpr (WINT) {
+      const PackedTable tbl{reinterpret_cast<unsigned long long*>(D.arena_vals), 0u, 0u};
+      best = cand_scan<WINT>(D, x, tbl, c * kHubChunk + threadIdx.x, (c + 1) * kHubChunk, blockDim.x,
+                             self_v, lowest);
+    } else {
+      const SplitTable<Acc> tbl{D.arena_keys, const_cast<Acc*>(vals), 0u, 0u};
+      best = cand_scan<WINT>(D, x, tbl, c * kHubChunk + threadIdx.x, (c + 1) * kHubChunk, blockDim.x,
+                             self_v, lowest);
+    }
     best = block_max<256>(best, red);
     if (threadIdx.x == 0 && best) atomicMax(&D.map[pos], best);
   }
@@ -1489,6 +1511,33 @@ __global__ void k_hub_owner(int dslot, int bin) {
   }
 }
 
+// Insert into a community's global contraction table at arena offset `off` (capacity `cap`).
+template <bool WINT>
+__device__ __forceinline__ bool hub_table_add(const Dev& D, uint32_t off, uint32_t cap, uint32_t d,
+                                              typename WTraits<WINT>::Acc w) {
+  using Acc = typename WTraits<WINT>::Acc;
+  const uint32_t mask = cap - 1u, shift = 32u - log2_pow2(cap);
+  if constexpr (WINT) {
+    return PackedTable{reinterpret_cast<unsigned long long*>(D.arena_vals) + off, mask, shift}.add(d, w);
+  } else {
+    return table_add(D.arena_keys + off, reinterpret_cast<Acc*>(D.arena_vals) + off, mask, shift, d, w);
+  }
+}
+// Slot `i` of the arena: its community (kEmpty if unused) and sum.
+template <bool WINT>
+__device__ __forceinline__ void hub_table_load(const Dev& D, uint32_t i, uint32_t& key,
+                                               typename WTraits<WINT>::Acc& sum) {
+  using Acc = typename WTraits<WINT>::Acc;
+  if constexpr (WINT) {
+    const unsigned long long x = reinterpret_cast<const unsigned long long*>(D.arena_vals)[i];
+    key = (uint32_t)(x >> 32);
+    sum = (Acc)(uint32_t)x;
+  } else {
+    key = D.arena_keys[i];
+    sum = key != kEmpty ? reinterpret_cast<const Acc*>(D.arena_vals)[i] : Acc(0);
+  }
+}
+
 // Bin-7 insert: one warp per member vertex, all members of all large communities at once,
 // into their communities' global tables (L2 atomics).
 template <bool WINT>
@@ -1500,7 +1549,6 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
-  Acc* vals = reinterpret_cast<Acc*>(D.arena_vals);
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1528,8 +1576,7 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
     const uint32_t g = D.gid ? D.gid[D.col[e]] : 0u;
     const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
-    if (!table_add(D.arena_keys + off, vals + off, cap - 1u, 32u - log2_pow2(cap), d, (Acc)w[e]))
-      err |= kErrTableFull;
+    if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
   };
   for (uint32_t vb = warp * 32u; vb < n; vb += nwarps * 32u) {
     const uint32_t v = vb + lane;
@@ -1574,7 +1621,6 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
   Ctrl* C = D.ctrl;
   const uint32_t count = C->long_count;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
-  Acc* vals = reinterpret_cast<Acc*>(D.arena_vals);
   uint32_t err = 0;
   const uint32_t n = C->n, n2 = C->n_next;
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
@@ -1590,14 +1636,13 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
     const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     if (off == kEmpty || (unsigned long long)off + cap > C->arena_slots) { err |= kErrIndex; continue; }
-    const uint32_t mask = cap - 1u, shift = 32u - log2_pow2(cap);
     const uint32_t rs = D.row[v] + piece * kHubPiece;
     const uint32_t re = min(D.row[v + 1], rs + kHubPiece);
     Acc self_acc = Acc(0);
     for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
       const uint32_t d = D.new_comm[D.col[e]];
       if (d == s) { self_acc += (Acc)w[e]; continue; }
-      if (!table_add(D.arena_keys + off, vals + off, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+      if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
     }
     self_acc = block_sum<256>(self_acc, sh);
     if (threadIdx.x == 0 && self_acc != Acc(0)) {
@@ -1621,7 +1666,6 @@ __global__ void __launch_bounds__(512) k_hub_emit(int dslot) {
   __shared__ double shd[33];
   __shared__ uint32_t base_sh;
   Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
-  const Acc* vals = reinterpret_cast<const Acc*>(D.arena_vals);
   constexpr int PER = kHubChunk / 512;
   for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const uint32_t s = D.hub_owner[c];
@@ -1630,8 +1674,13 @@ __global__ void __launch_bounds__(512) k_hub_emit(int dslot) {
     const uint32_t g = D.gid ? D.gid[v0] : 0u;
     const uint32_t slot0 = c * kHubChunk + threadIdx.x * PER;
     uint32_t cnt = 0;
+    uint32_t kk[PER];
+    Acc ss[PER];
 #pragma unroll
-    for (int i = 0; i < PER; ++i) cnt += D.arena_keys[slot0 + i] != kEmpty;
+    for (int i = 0; i < PER; ++i) {
+      hub_table_load<WINT>(D, slot0 + i, kk[i], ss[i]);
+      cnt += kk[i] != kEmpty;
+    }
     uint32_t total;
     uint32_t off = block_excl_scan<uint32_t, 512>(cnt, shu, &total);
     if (threadIdx.x == 0) base_sh = total ? atomicAdd(&D.newdeg[s], total) : 0u;
@@ -1640,9 +1689,9 @@ __global__ void __launch_bounds__(512) k_hub_emit(int dslot) {
     double ksum = 0.0, self = 0.0;
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-      const uint32_t d = D.arena_keys[slot0 + i];
+      const uint32_t d = kk[i];
       if (d == kEmpty) continue;
-      const Acc sum = vals[slot0 + i];
+      const Acc sum = ss[i];
       Wt wv;
       if (WINT) wv = (Wt)sum;
       else wv = (Wt)__double2float_rn((double)sum);
@@ -2050,15 +2099,13 @@ __global__ void k_agg_clear_next(int dslot) {
   }
 }
 // The global contraction tables of this aggregation: empty keys, zero values.
+template <bool WINT>
 __global__ void k_arena_clear(int dslot) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t used = min(C->hub_cursor, C->arena_slots);
-  unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < used; s += gridDim.x * blockDim.x) {
-    D.arena_keys[s] = kEmpty;
-    vals[s] = 0ull;
-  }
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < used; s += gridDim.x * blockDim.x)
+    arena_clear_slot<WINT>(D, s);
 }
 // Level body entry: the pass loop runs while some graph iterates.
 __global__ void k_gate_pass(int dslot, GraphCtl gc) {
