@@ -317,6 +317,39 @@ struct PackedTable {
   }
 };
 
+// A shared-memory table in the layout of the weight mode: packed slots for integer weights,
+// split key / sum arrays for fp32 weights (both 4 + sizeof(sum) bytes per slot on average).
+template <bool WINT>
+struct ScratchTable {
+  using Acc = typename WTraits<WINT>::Acc;
+  uint32_t* keys;              // split layout
+  Acc* vals;
+  unsigned long long* slots;   // packed layout
+  uint32_t mask, shift;
+  __device__ __forceinline__ void clear(uint32_t i) const {
+    if constexpr (WINT) {
+      slots[i] = kEmptySlot;
+    } else {
+      keys[i] = kEmpty;
+      vals[i] = Acc(0);
+    }
+  }
+  __device__ __forceinline__ bool add(uint32_t c, Acc w) const {
+    if constexpr (WINT) return PackedTable{slots, mask, shift}.add(c, w);
+    else return table_add(keys, vals, mask, shift, c, w);
+  }
+  __device__ __forceinline__ void load(uint32_t i, uint32_t& k, Acc& v) const {
+    if constexpr (WINT) {
+      const unsigned long long x = slots[i];
+      k = (uint32_t)(x >> 32);
+      v = (uint32_t)x;
+    } else {
+      k = keys[i];
+      v = vals[i];
+    }
+  }
+};
+
 // ---- warp / block reductions -------------------------------------------------------------------
 template <int T>
 __device__ __forceinline__ unsigned long long team_max(unsigned long long x, unsigned mask) {

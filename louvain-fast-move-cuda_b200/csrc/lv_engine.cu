@@ -355,9 +355,9 @@ class Run {
     team_grid<32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     const size_t bsmem = (size_t)block_cap * (4 + acc_size());
-    ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI, false>, bsmem);
+    ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, bsmem);
-    grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI, false>, 512, bsmem));
+    grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI>, 512, bsmem));
   }
 
   // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
@@ -628,7 +628,7 @@ class Run {
     k_opt_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
     k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
-    k_opt_block<WI, false><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
+    k_opt_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
     k_opt_hub_prep<WI><<<ctx->sms * 4, 256, 0, st>>>(Dd);
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);

@@ -414,16 +414,26 @@ __global__ void __launch_bounds__(256) k_opt_team(int dslot, int bin, uint32_t c
     } else {
       const uint32_t cap_v = live ? table_cap(x.re - x.rs, x.ng) : 2u;
       const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
-      if (live)
-        for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
-      __syncwarp();
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
-      const SplitTable<Acc> tbl{keys, vals, mask, shift};
-      if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, tbl, self_acc, err);
-      self_acc = team_sum<T>(self_acc);
-      __syncwarp();
-      if (live) best = cand_scan<WINT>(D, x, tbl, lane, cap_v, T, Tr::to_float(self_acc), lowest);
+      auto table_pass = [&](const auto& tbl) {
+        __syncwarp();
+        if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, tbl, self_acc, err);
+        self_acc = team_sum<T>(self_acc);
+        __syncwarp();
+        if (live) best = cand_scan<WINT>(D, x, tbl, lane, cap_v, T, Tr::to_float(self_acc), lowest);
+      };
+      if constexpr (WINT) {
+        // integer weights: packed (community << 32 | sum) slots, 8 bytes like the split pair
+        unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
+        if (live)
+          for (uint32_t s = lane; s < cap_v; s += T) slots[s] = kEmptySlot;
+        table_pass(PackedTable{slots, mask, shift});
+      } else {
+        if (live)
+          for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
+        table_pass(SplitTable<Acc>{keys, vals, mask, shift});
+      }
       best = team_max<T>(best, kFull);
       __syncwarp();
     }
@@ -476,10 +486,9 @@ __device__ __forceinline__ unsigned long long block_max(unsigned long long x, un
 }
 
 // ---- pass: optimisation, one block per high-degree vertex ----------------------------------------
-// GTABLE = false: the table lives in shared memory (capacity `cap` slots); true: the table is
-// a slice of the global arena at hub_off[idx] (vertices whose 2x degree exceeds shared
-// memory), touched through L2 atomics.
-template <bool WINT, bool GTABLE>
+// The vertex's table lives in shared memory (capacity `cap` slots; vertices whose table would
+// not fit are in bin 7, handled by the k_opt_hub_* kernels).
+template <bool WINT>
 __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
@@ -505,28 +514,27 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
     } else {
       const uint32_t cap_v = table_cap(x.re - x.rs, x.ng);
       const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
-      uint32_t* keys;
-      Acc* vals;
-      bool ok = true;
-      if (GTABLE) {
-        const uint32_t off = D.hub_off[idx];
-        ok = (unsigned long long)off + cap_v <= C->arena_slots;
-        keys = D.arena_keys + off;
-        vals = reinterpret_cast<Acc*>(D.arena_vals) + off;
-      } else {
-        ok = cap_v <= cap;
-        keys = reinterpret_cast<uint32_t*>(smem);
-        vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
-      }
+      const bool ok = cap_v <= cap;
       if (!ok) err |= kErrArena;
-      if (ok)
-        for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
-      __syncthreads();
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
-      const SplitTable<Acc> tbl{keys, vals, mask, shift};
-      if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, tbl, self_acc, err);
-      self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
-      if (ok) best = cand_scan<WINT>(D, x, tbl, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
+      auto table_pass = [&](const auto& tbl) {
+        __syncthreads();
+        if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, tbl, self_acc, err);
+        self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
+        if (ok) best = cand_scan<WINT>(D, x, tbl, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
+      };
+      if constexpr (WINT) {
+        unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
+        if (ok)
+          for (uint32_t s = threadIdx.x; s < cap_v; s += NT) slots[s] = kEmptySlot;
+        table_pass(PackedTable{slots, mask, shift});
+      } else {
+        uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
+        Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
+        if (ok)
+          for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
+        table_pass(SplitTable<Acc>{keys, vals, mask, shift});
+      }
     }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best) {
@@ -1772,9 +1780,10 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     CommCtx x{};
     if (live) x = load_comm(D, s);
     const uint32_t cap_v = live ? contract_cap(x.dsum, D.gs[x.g].n_next, false) : 2u;
-    const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+    const ScratchTable<WINT> tbl{keys, vals, reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap,
+                                 cap_v - 1u, 32u - log2_pow2(cap_v)};
     if (live)
-      for (uint32_t i = lane; i < cap_v; i += T) { keys[i] = kEmpty; vals[i] = Acc(0); }
+      for (uint32_t i = lane; i < cap_v; i += T) tbl.clear(i);
     __syncwarp();
     // entries staying inside the community (the new self-loop, the hottest key) are summed in
     // registers; only entries to other communities go through the table
@@ -1782,7 +1791,7 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     auto add = [&](uint32_t e, uint32_t, uint32_t) {
       const uint32_t d = D.new_comm[D.col[e]];
       if (d == s) { self_acc += (Acc)w[e]; return; }
-      if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+      if (!tbl.add(d, (Acc)w[e])) err |= kErrTableFull;
     };
     if (T == 32) {
       // a warp per community: members taken 32 at a time, their entries spread over all lanes
@@ -1810,7 +1819,12 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     uint32_t cnt = 0;
     double ksum = 0.0;
     if (live)
-      for (uint32_t i = lane; i < cap_v; i += T) cnt += keys[i] != kEmpty;
+      for (uint32_t i = lane; i < cap_v; i += T) {
+        uint32_t d;
+        Acc sum;
+        tbl.load(i, d, sum);
+        cnt += d != kEmpty;
+      }
     uint32_t off = cnt;
 #pragma unroll
     for (int o = 1; o < T; o <<= 1) {
@@ -1821,9 +1835,10 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     off -= cnt;
     if (live) {
       for (uint32_t i = lane; i < cap_v; i += T) {
-        const uint32_t d = keys[i];
+        uint32_t d;
+        Acc sum;
+        tbl.load(i, d, sum);
         if (d == kEmpty) continue;
-        const Acc sum = vals[i];
         Wt wv;
         if (WINT) wv = (Wt)sum;
         else wv = (Wt)__double2float_rn((double)sum);
@@ -1878,25 +1893,21 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
     const uint32_t s = list[idx];
     const CommCtx x = load_comm(D, s);
     const uint32_t cap_v = contract_cap(x.dsum, D.gs[x.g].n_next, false);
-    const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
-    uint32_t* keys;
-    Acc* vals;
-    bool ok;
-    {
-      ok = cap_v <= cap;
-      keys = reinterpret_cast<uint32_t*>(smem);
-      vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
-    }
+    const bool ok = cap_v <= cap;
+    const ScratchTable<WINT> tbl{reinterpret_cast<uint32_t*>(smem),
+                                 reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t)),
+                                 reinterpret_cast<unsigned long long*>(smem), cap_v - 1u,
+                                 32u - log2_pow2(cap_v)};
     if (!ok) err |= kErrArena;
     if (ok)
-      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) { keys[i] = kEmpty; vals[i] = Acc(0); }
+      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) tbl.clear(i);
     __syncthreads();
     Acc self_acc = Acc(0);  // entries staying inside the community, kept out of the table
     if (ok) {
       auto add = [&](uint32_t e, uint32_t, uint32_t) {
         const uint32_t d = D.new_comm[D.col[e]];
         if (d == s) { self_acc += (Acc)w[e]; return; }
-        if (!table_add(keys, vals, mask, shift, d, (Acc)w[e])) err |= kErrTableFull;
+        if (!tbl.add(d, (Acc)w[e])) err |= kErrTableFull;
       };
       // members taken NT at a time; their entries spread evenly over the whole block, each
       // thread finding its entry's member by binary search in shared memory
@@ -1928,15 +1939,21 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
     self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(shd));
     uint32_t cnt = 0;
     if (ok)
-      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) cnt += keys[i] != kEmpty;
+      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) {
+        uint32_t d;
+        Acc sum;
+        tbl.load(i, d, sum);
+        cnt += d != kEmpty;
+      }
     uint32_t total;
     uint32_t off = block_excl_scan<uint32_t, NT>(cnt, shu, &total);
     double ksum = 0.0;
     if (ok) {
       for (uint32_t i = threadIdx.x; i < cap_v; i += NT) {
-        const uint32_t d = keys[i];
+        uint32_t d;
+        Acc sum;
+        tbl.load(i, d, sum);
         if (d == kEmpty) continue;
-        const Acc sum = vals[i];
         Wt wv;
         if (WINT) wv = (Wt)sum;
         else wv = (Wt)__double2float_rn((double)sum);
