@@ -104,6 +104,7 @@ struct Ctrl {
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
   uint32_t long_count;         // aggregation: pieces of long rows for k_hub_insert_long
   uint32_t long_movers;        // pass: team-kernel movers with long rows, for k_apply_long
+  uint32_t hub_members;        // aggregation: members of the bin-7 communities, for k_hub_insert
   uint32_t hub_items;          // pass: pieces of the bin-7 (global-table) vertices' rows
   uint32_t apply_items;        // pass: pieces of the rows of movers found by block kernels
   uint32_t hub_cursor;         // global hash-table arena cursor (slots)
@@ -389,6 +390,34 @@ __device__ __forceinline__ void warp_expand_rows(uint32_t rs, uint32_t len, uint
     const uint32_t base = __shfl_sync(kFull, rs, k) - __shfl_sync(kFull, excl, k);
     const uint32_t a = __shfl_sync(kFull, pa, k), b = __shfl_sync(kFull, pb, k);
     if (j < total) f(base + j, a, b);
+  }
+}
+
+// The same with three payload words per row: f(entry index, pa, pb, pc).
+template <class F>
+__device__ __forceinline__ void warp_expand_rows3(uint32_t rs, uint32_t len, uint32_t pa, uint32_t pb,
+                                                  uint32_t pc, F&& f) {
+  const int lane = threadIdx.x & 31;
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t excl = incl - len;
+  for (uint32_t jb = 0; jb < total; jb += 32) {
+    const uint32_t j = jb + lane;
+    int k = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const uint32_t ex = __shfl_sync(kFull, excl, k + step);
+      if (ex <= j) k += step;
+    }
+    const uint32_t base = __shfl_sync(kFull, rs, k) - __shfl_sync(kFull, excl, k);
+    const uint32_t a = __shfl_sync(kFull, pa, k), b = __shfl_sync(kFull, pb, k),
+                   c = __shfl_sync(kFull, pc, k);
+    if (j < total) f(base + j, a, b, c);
   }
 }
 

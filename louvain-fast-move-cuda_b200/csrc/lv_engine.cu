@@ -466,7 +466,6 @@ class Run {
     D.comm = dalloc<uint32_t>(ctx, owned, n);
     D.a = dalloc<double>(ctx, owned, n);
     D.new_comm = dalloc<uint32_t>(ctx, owned, n);
-    D.moved_it = dalloc<uint32_t>(ctx, owned, n);
     D.active_it = dalloc<uint32_t>(ctx, owned, n);
     for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n);
     D.hub_off = dalloc<uint32_t>(ctx, owned, n);
@@ -695,6 +694,7 @@ class Run {
     // the largest new communities: many blocks insert into their global tables
     k_arena_clear<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(Dd, kNumBins - 1);
+    k_hub_member_prefix<<<1, 1024, 0, st>>>(Dd);
     k_hub_insert<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_hub_insert_long<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_hub_emit<WI><<<ctx->sms * 8, 512, 0, st>>>(Dd);
@@ -707,7 +707,7 @@ class Run {
     k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     scan<uint32_t, false, kScanDeg>();
     k_agg_compact<WI><<<grid_n, 256, 0, st>>>(Dd);
-    launches += 13;
+    launches += 14;
   }
   void agg_tail() {
     k_agg_best<<<grid_n, 256, 0, st>>>(Dd);

@@ -27,7 +27,6 @@ struct Dev {
   uint32_t* comm;       // [n] communities
   double* a;            // [n] communities_weight
   uint32_t* new_comm;   // [n] target of this pass's move
-  uint32_t* moved_it;   // [n] pass stamp of the last move
   uint32_t* active_it;  // [n] pass stamp for which the vertex is active
   uint32_t* bins[kNumBins];
   uint32_t* hub_off;    // [n] arena offset per entry of the global-table bin
@@ -210,7 +209,6 @@ __device__ __forceinline__ void emit_move(const Dev& D, bool move, uint32_t v, u
   base = __shfl_sync(kFull, base, leader);
   if (move) {
     D.new_comm[v] = c;
-    D.moved_it[v] = it;
     D.movers[base + __popc(mask & lanemask_lt())] = v;
   }
 }
@@ -221,7 +219,6 @@ __device__ __forceinline__ void emit_hub_move(const Dev& D, uint32_t v, uint32_t
                                               uint32_t d) {
   Ctrl* C = D.ctrl;
   D.new_comm[v] = c;
-  D.moved_it[v] = it;
   D.movers[C->n - 1u - atomicAdd(&C->hub_mover_count, 1u)] = v;
   const uint32_t np = (d + kHubPiece - 1) / kHubPiece;
   const uint32_t p0 = atomicAdd(&C->apply_items, np);
@@ -697,7 +694,7 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   // kBatch entries per lane at a time: their gathers are issued before any is used
   for (uint32_t e = e0; e < re; e += kBatch * step) {
-    uint32_t uu[kBatch], pre[kBatch], mv[kBatch];
+    uint32_t uu[kBatch], pre[kBatch], nc[kBatch];
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       const uint32_t ek = e + k * step;
@@ -706,14 +703,15 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       pre[k] = uu[k] != kEmpty ? D.comm[uu[k]] : 0u;
-      mv[k] = uu[k] != kEmpty ? D.moved_it[uu[k]] : 0u;
+      nc[k] = uu[k] != kEmpty ? D.new_comm[uu[k]] : 0u;
     }
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       if (uu[k] == kEmpty) continue;
       const uint32_t u = uu[k];
-      const bool mu = mv[k] == it;
-      const uint32_t post = mu ? D.new_comm[u] : pre[k];
+      // new_comm equals comm for every vertex that did not move this pass
+      const bool mu = nc[k] != pre[k];
+      const uint32_t post = nc[k];
       if (post != nw) D.active_it[u] = it + 1;
       const int dd = (int)(nw == post) - (int)(old == pre[k]);
       if (dd) {
@@ -792,7 +790,7 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t excl = incl - len;
     for (uint32_t jb = 0; jb < total; jb += 32u * kBatch) {
-      uint32_t ee[kBatch], oo[kBatch], nn[kBatch], uu[kBatch], pre[kBatch], mv[kBatch];
+      uint32_t ee[kBatch], oo[kBatch], nn[kBatch], uu[kBatch], pre[kBatch], nc[kBatch];
 #pragma unroll
       for (int q = 0; q < kBatch; ++q) {
         const uint32_t j = jb + (uint32_t)q * 32u + lane;
@@ -810,14 +808,14 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
 #pragma unroll
       for (int q = 0; q < kBatch; ++q) {
         pre[q] = uu[q] != kEmpty ? D.comm[uu[q]] : 0u;
-        mv[q] = uu[q] != kEmpty ? D.moved_it[uu[q]] : 0u;
+        nc[q] = uu[q] != kEmpty ? D.new_comm[uu[q]] : 0u;
       }
 #pragma unroll
       for (int q = 0; q < kBatch; ++q) {
         if (uu[q] == kEmpty) continue;
         const uint32_t u = uu[q];
-        const bool mu = mv[q] == it;
-        const uint32_t post = mu ? D.new_comm[u] : pre[q];
+        const bool mu = nc[q] != pre[q];  // new_comm equals comm unless u moved this pass
+        const uint32_t post = nc[q];
         if (post != nn[q]) D.active_it[u] = it + 1;
         const int dd = (int)(nn[q] == post) - (int)(oo[q] == pre[q]);
         if (dd) {
@@ -1097,10 +1095,12 @@ __global__ void k_level_init(int dslot) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     if (D.gs[g].phase != kIterating) continue;
+    // new_comm == comm marks "did not move" for the apply kernels (movers get new_comm != comm
+    // and k_commit_sq copies it back), so it starts equal too
     D.comm[v] = v;
+    D.new_comm[v] = v;
     D.a[v] = D.k[v];
     D.active_it[v] = it;
-    D.moved_it[v] = kNever;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->mover_count = 0;
@@ -1546,8 +1546,32 @@ __device__ __forceinline__ void hub_table_load(const Dev& D, uint32_t i, uint32_
   }
 }
 
-// Bin-7 insert: one warp per member vertex, all members of all large communities at once,
-// into their communities' global tables (L2 atomics).
+// Where the members of each bin-7 community start among all bin-7 members (exclusive prefix of
+// their member counts, in `rank`, which is free after the scatter) and how many there are.
+__global__ void __launch_bounds__(1024) k_hub_member_prefix(int dslot) {
+  const Dev& D = c_dev[dslot];
+  __shared__ uint32_t sh[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->bin_count[kNumBins - 1];
+  uint32_t run = 0;
+  for (uint32_t base = 0; base < count; base += 1024) {
+    const uint32_t idx = base + threadIdx.x;
+    uint32_t m = 0;
+    if (idx < count) {
+      const uint32_t s = D.bins[kNumBins - 1][idx];
+      m = (uint32_t)(D.cd[s + 1] >> 32) - (uint32_t)(D.cd[s] >> 32);
+    }
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan<uint32_t, 1024>(m, sh, &tot);
+    if (idx < count) D.rank[idx] = run + ex;
+    run += tot;
+  }
+  if (threadIdx.x == 0) C->hub_members = run;
+}
+
+// Bin-7 insert: the members of all large communities at once (and no other vertex), 32 per
+// warp, their rows spread over the lanes, into their communities' global tables (L2 atomics).
+// Long rows go to k_hub_insert_long in pieces.
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
   const Dev& D = c_dev[dslot];
@@ -1555,14 +1579,14 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
   Ctrl* C = D.ctrl;
-  const uint32_t n = C->n;
+  const uint32_t count = C->bin_count[kNumBins - 1], total = C->hub_members;
+  const uint32_t* hubs = D.bins[kNumBins - 1];
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t err = 0;
-  // a warp takes 32 consecutive vertices; the rows of those in large communities are spread
-  // over its lanes. Entries staying inside their community are summed in registers.
+  // entries staying inside their community are summed in registers
   uint32_t self_s = kEmpty;  // per-lane running self-loop sum, flushed when the community changes
   Acc self_acc = Acc(0);
   auto flush_self = [&]() {
@@ -1570,7 +1594,7 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
     if (WINT) atomicAdd(&D.hubself[self_s], (unsigned long long)self_acc);
     else atomicAdd(reinterpret_cast<double*>(&D.hubself[self_s]), (double)self_acc);
   };
-  auto add = [&](uint32_t e, uint32_t s, uint32_t off) {
+  auto add = [&](uint32_t e, uint32_t s, uint32_t off, uint32_t cap) {
     const uint32_t d = D.new_comm[D.col[e]];
     if (d == s) {
       if (s != self_s) {
@@ -1581,38 +1605,38 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
       self_acc += (Acc)w[e];
       return;
     }
-    const uint32_t g = D.gid ? D.gid[D.col[e]] : 0u;
-    const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
-    const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
   };
-  for (uint32_t vb = warp * 32u; vb < n; vb += nwarps * 32u) {
-    const uint32_t v = vb + lane;
-    uint32_t rs = 0, len = 0, s = 0, off = kEmpty;
-    if (v < n) {
+  for (uint32_t pb = warp * 32u; pb < total; pb += nwarps * 32u) {
+    const uint32_t p = pb + lane;
+    uint32_t rs = 0, len = 0, s = 0, off = 0, cap = 0;
+    if (p < total) {
+      uint32_t lo = 0, hi = count;  // last community whose members start at or before p
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (D.rank[mid] <= p) lo = mid; else hi = mid;
+      }
+      s = hubs[lo];
+      const unsigned long long a = D.cd[s], b = D.cd[s + 1];
+      const uint32_t v = D.members[(uint32_t)(a >> 32) + (p - D.rank[lo])];
       const uint32_t g = D.gid ? D.gid[v] : 0u;
-      if (D.gs[g].cont) {
-        s = D.new_comm[v];
-        off = D.hubtab[s];
-        if (off != kEmpty) {
-          const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
-          const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
-          if ((unsigned long long)off + cap > C->arena_slots) err |= kErrArena;
-          else {
-            rs = D.row[v];
-            len = D.row[v + 1] - rs;
-            if (len > kHubLongRow) {
-              // long rows are cut into pieces that separate blocks insert (k_hub_insert_long)
-              const uint32_t np = (len + kHubPiece - 1) / kHubPiece;
-              const uint32_t p0 = atomicAdd(&C->long_count, np);
-              for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
-              len = 0;
-            }
-          }
+      off = D.hub_off[lo];
+      cap = contract_cap((uint32_t)b - (uint32_t)a, D.gs[g].n_next, true);
+      if ((unsigned long long)off + cap > C->arena_slots) {
+        err |= kErrArena;
+      } else {
+        rs = D.row[v];
+        len = D.row[v + 1] - rs;
+        if (len > kHubLongRow) {
+          // long rows are cut into pieces that separate blocks insert (k_hub_insert_long)
+          const uint32_t np = (len + kHubPiece - 1) / kHubPiece;
+          const uint32_t p0 = atomicAdd(&C->long_count, np);
+          for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
+          len = 0;
         }
       }
     }
-    warp_expand_rows(rs, len, s, off, add);
+    warp_expand_rows3(rs, len, s, off, cap, add);
   }
   flush_self();
   if (err) atomicOr(&C->err, err);
