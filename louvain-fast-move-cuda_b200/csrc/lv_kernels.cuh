@@ -379,7 +379,7 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 // they enter the argmax (the reference's own-community and negative candidates can never
 // win a move).
 template <int T, bool WINT>
-__global__ void __launch_bounds__(256) k_opt_team(int dslot, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
