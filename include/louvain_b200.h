@@ -230,6 +230,28 @@ lv_status lv_community_get_trace(lv_community* c, lv_trace_record* out, int32_t 
 lv_status lv_modularity_noalloc(int64_t n, const int64_t* row_ptr, const int32_t* col, const float* w,
                                 const int32_t* comm, int32_t weights_integer, double* out, void* stream);
 
+/* ---- edge-list ingest --------------------------------------------------------------------
+ * GraphHost(name, weighted = false, skip_line) (graph.cu:17-87, graph.cuh:60-91) on the GPU:
+ * `text` is the file's bytes (host or device memory). The first `skip_line` lines are skipped;
+ * the rest is read as whitespace-separated integers taken in pairs, ending at the first token
+ * that is not an integer (an unpaired last token is dropped); distinct unordered pairs become
+ * edges (a self-loop pair included), ids are renumbered as id - min_id and must be contiguous.
+ * The result is the symmetric CSR the reference's GraphDevice holds (both directions, a
+ * self-loop stored twice, rows sorted), kept on the device. Errors: LV_ERR_INPUT (no pair,
+ * ids not contiguous), LV_ERR_RANGE (too large). */
+typedef struct lv_ingest lv_ingest;
+lv_status lv_ingest_edge_list(lv_context* ctx, const char* text, int64_t len, int32_t skip_line,
+                              int32_t in_mem, lv_ingest** out);
+/* n_nodes, n_links (graphHost.cuh:8-9), CSR entries (2 n_links), min_id (graphHost.cuh:11). */
+lv_status lv_ingest_info(const lv_ingest* g, int64_t* n_nodes, int64_t* n_links, int64_t* entries,
+                         int64_t* min_id);
+/* row_ptr int64[n_nodes + 1], col int32[entries], into host or device memory. */
+lv_status lv_ingest_copy_csr(const lv_ingest* g, int64_t* row_ptr, int32_t* col, int32_t out_mem);
+/* lv_run_csr on the ingested graph without leaving the device. */
+lv_status lv_ingest_run(lv_ingest* g, int32_t* out_comm, int32_t out_mem, double* out_modularity,
+                        lv_stats* stats);
+lv_status lv_ingest_destroy(lv_ingest* g);
+
 /* ---- serving ---------------------------------------------------------------------------
  * Continuous batching with graph state resident in HBM. No reference counterpart.
  * Requests are admitted while the device memory they need fits `budget_bytes` and a slot is

@@ -103,6 +103,7 @@ EXPORTS = (
     "lv_community_get_best", "lv_community_get_graph", "lv_community_get_trace",
     "lv_server_create", "lv_server_destroy", "lv_server_submit", "lv_server_submit_borrowed",
     "lv_server_progress", "lv_server_poll", "lv_server_drain",
+    "lv_ingest_edge_list", "lv_ingest_info", "lv_ingest_copy_csr", "lv_ingest_run", "lv_ingest_destroy",
 )
 
 
@@ -146,6 +147,11 @@ def load_library(path: Optional[str] = None):
         "lv_server_progress": (i32, [vp, P(i64), P(i64), P(i64)]),
         "lv_server_poll": (i32, [vp, i64, vp, P(dbl), P(dbl), P(i32)]),
         "lv_server_drain": (i32, [vp]),
+        "lv_ingest_edge_list": (i32, [vp, vp, i64, i32, i32, P(vp)]),
+        "lv_ingest_info": (i32, [vp, P(i64), P(i64), P(i64), P(i64)]),
+        "lv_ingest_copy_csr": (i32, [vp, vp, vp, i32]),
+        "lv_ingest_run": (i32, [vp, vp, i32, P(dbl), P(Stats)]),
+        "lv_ingest_destroy": (i32, [vp]),
     }
     missing = []
     for name, (res, args) in sig.items():
@@ -287,6 +293,11 @@ class Engine:
         self.cfg = out
         return list(out.bin_max_degree), ms.value
 
+    def ingest(self, source, skip_line: int = 0) -> "Ingest":
+        """lv_ingest_edge_list: an edge-list file (path) or its bytes parsed into a CSR on the
+        GPU with the reference's GraphHost rules (graph.cu:17-87)."""
+        return Ingest(self, source, skip_line)
+
     def community(self, g: CSRGraph) -> "CommunityState":
         return CommunityState(self, g)
 
@@ -371,6 +382,51 @@ class CommunityState:
         self.e.check(self.e._L.lv_community_get_trace(self._h, out.ctypes.data, cap, ctypes.byref(ln)),
                      "lv_community_get_trace")
         return out[: min(ln.value, cap)]
+
+
+class Ingest:
+    """A graph read on the GPU from edge-list text (lv_ingest_*): n_nodes, n_links, min_id,
+    the CSR (``csr()``) and Louvain on it without leaving the device (``run()``)."""
+
+    def __init__(self, engine: Engine, source, skip_line: int = 0):
+        self.e = engine
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            data = bytes(source)
+        else:
+            with open(source, "rb") as f:
+                data = f.read()
+        buf = ctypes.create_string_buffer(data, len(data))
+        h = ctypes.c_void_p()
+        engine.check(engine._L.lv_ingest_edge_list(engine._h, buf, len(data), int(skip_line), MEM_HOST,
+                                                   ctypes.byref(h)), "lv_ingest_edge_list")
+        self._h = h
+        n, m, E, mn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        engine._L.lv_ingest_info(h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(E), ctypes.byref(mn))
+        self.n_nodes, self.n_links, self.entries, self.min_id = n.value, m.value, E.value, mn.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.e._L.lv_ingest_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def csr(self) -> CSRGraph:
+        row = np.empty(self.n_nodes + 1, dtype=np.int64)
+        col = np.empty(self.entries, dtype=np.int32)
+        self.e.check(self.e._L.lv_ingest_copy_csr(self._h, row.ctypes.data, col.ctypes.data, MEM_HOST),
+                     "lv_ingest_copy_csr")
+        return CSRGraph(n=self.n_nodes, row_ptr=row, col=col, w=None, name="ingested")
+
+    def run(self):
+        """(communities, modularity, Stats) of a Louvain run on the ingested graph."""
+        out = np.empty(self.n_nodes, dtype=np.int32)
+        q = ctypes.c_double(0)
+        st = Stats()
+        self.e.check(self.e._L.lv_ingest_run(self._h, out.ctypes.data, MEM_HOST, ctypes.byref(q),
+                                             ctypes.byref(st)), "lv_ingest_run")
+        return out, q.value, st
 
 
 class Server:

@@ -1437,3 +1437,4 @@ lv_status lv_run_batch(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_off
 }  // extern "C"
 
 #include "lv_server.cuh"
+#include "lv_ingest.cuh"
