@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one untimed run on the device-resident graph (for profilers), then exit")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "batched", "served"],
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batched", "served", "ingest"],
                     help="rmat: the single R-MAT graph (default line); batched: 4,096 uneven "
                          "Chung-Lu graphs in one batch against a loop of single runs; served: "
                          "Poisson request stream through the server against a loop")
@@ -422,6 +422,59 @@ def run_served(args, local):
     return 0
 
 
+def run_ingest(args, local):
+    """Edge-list text to CSR: the raw R-MAT pairs of the workload (duplicates and self-loops
+    included, ids renumbered to be contiguous) as `u v` lines, read on the GPU with the
+    reference's GraphHost rules (lv_ingest_*), text already in host memory; the CPU loader
+    (oracle/edge_list.py, numpy) on a bounded sample of the same generator beside it."""
+    import importlib
+    import torch
+    lv = importlib.import_module(PKG)
+    graphs = importlib.import_module(PKG + ".graphs")
+    torch.cuda.set_device(local)
+
+    def text_for(scale):
+        u, v = graphs.rmat_pairs(scale, EDGE_FACTOR, seed=SEED)
+        ids, inv = np.unique(np.concatenate([u, v]), return_inverse=True)
+        return graphs.edge_list_bytes(inv[: u.size], inv[u.size:])
+
+    text = np.frombuffer(text_for(args.scale), dtype=np.uint8)
+    pinned = torch.from_numpy(text.copy()).pin_memory().numpy()
+    eng = lv.Engine(local)
+    for _ in range(max(1, args.warmup)):
+        eng.ingest(pinned).close()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g = eng.ingest(pinned)
+        times.append(time.perf_counter() - t0)
+        info = (g.n_nodes, g.n_links)
+        g.close()
+    sec = min(times)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import edge_list as O
+    s_scale = args.cpu_sample_scale - 1
+    sample = text_for(s_scale)
+    t0 = time.perf_counter()
+    n_s, nl_s, _, _, _ = O.graph_host_csr(sample)
+    cpu_sec = time.perf_counter() - t0
+    line = {
+        "metric": "ingest_edges_per_s", "value": info[1] / sec, "unit": "edges/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 ids",
+        "data": "synthetic",
+        "config": {"workload": f"rmat_s{args.scale}_ef16_raw_edge_list", "bytes": int(text.size),
+                   "lines": int(EDGE_FACTOR << args.scale), "n_nodes": info[0], "n_links": info[1]},
+        "text_gb_per_s": text.size / sec / 1e9,
+        "cpu_baseline": {"value": nl_s / cpu_sec, "unit": "edges/s", "cores": 1, "kind": "port",
+                         "sample": f"R-MAT scale {s_scale} raw edge list ({len(sample)} bytes, "
+                                   f"{nl_s} links), oracle/edge_list.py (numpy), {cpu_sec:.2f} s"},
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
@@ -435,6 +488,8 @@ def main():
         return run_batched(args, local) if rank == 0 else 0
     if args.workload == "served":
         return run_served(args, local) if rank == 0 else 0
+    if args.workload == "ingest":
+        return run_ingest(args, local) if rank == 0 else 0
 
     import importlib
     import torch

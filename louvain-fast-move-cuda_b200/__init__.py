@@ -390,14 +390,19 @@ class Ingest:
 
     def __init__(self, engine: Engine, source, skip_line: int = 0):
         self.e = engine
-        if isinstance(source, (bytes, bytearray, memoryview)):
-            data = bytes(source)
+        if isinstance(source, np.ndarray):  # the bytes in a uint8 array (read in place)
+            data = np.ascontiguousarray(source, dtype=np.uint8)
+            ptr, size = data.ctypes.data, data.size
         else:
-            with open(source, "rb") as f:
-                data = f.read()
-        buf = ctypes.create_string_buffer(data, len(data))
+            if isinstance(source, (bytes, bytearray, memoryview)):
+                raw = bytes(source)
+            else:
+                with open(source, "rb") as f:
+                    raw = f.read()
+            data = ctypes.create_string_buffer(raw, len(raw))
+            ptr, size = ctypes.addressof(data), len(raw)
         h = ctypes.c_void_p()
-        engine.check(engine._L.lv_ingest_edge_list(engine._h, buf, len(data), int(skip_line), MEM_HOST,
+        engine.check(engine._L.lv_ingest_edge_list(engine._h, ptr, size, int(skip_line), MEM_HOST,
                                                    ctypes.byref(h)), "lv_ingest_edge_list")
         self._h = h
         n, m, E, mn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -410,3 +410,39 @@ def rmat_device(n_target: int, edge_factor: int = 8, a: float = 0.57, b: float =
     u = (u * n_target) >> scale
     v = (v * n_target) >> scale
     return to_device_canonical(u, v, device=device, name=f"rmat_n{n_target}_ef{edge_factor}_s{seed}")
+
+
+def edge_list_bytes(u: np.ndarray, v: np.ndarray) -> bytes:
+    """``"u v\\n"`` lines for non-negative integer arrays, formatted with vectorised digit
+    extraction (no per-line Python work)."""
+    u = np.asarray(u, dtype=np.int64)
+    v = np.asarray(v, dtype=np.int64)
+    if u.size and min(int(u.min()), int(v.min())) < 0:
+        raise ValueError("non-negative ids only")
+
+    def ndig(x):
+        d = np.ones(x.shape, dtype=np.int64)
+        p = 10
+        for _ in range(18):
+            d += x >= p
+            p *= 10
+        return d
+
+    du, dv = ndig(u), ndig(v)
+    line = du + dv + 2
+    end = np.cumsum(line)
+    start = end - line
+    buf = np.empty(int(end[-1]) if end.size else 0, dtype=np.uint8)
+
+    def put(x, nd, first):
+        y = x.copy()
+        for k in range(int(nd.max()) if nd.size else 0):
+            m = k < nd
+            buf[(first + nd - 1 - k)[m]] = (y[m] % 10 + 48).astype(np.uint8)
+            y //= 10
+
+    put(u, du, start)
+    buf[start + du] = ord(" ")
+    put(v, dv, start + du + 1)
+    buf[end - 1] = ord("\n")
+    return buf.tobytes()
