@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--mode", default="SORT", choices=["SORT", "HASH"])
-    ap.add_argument("--cpu-sample-scale", type=int, default=19)
+    ap.add_argument("--cpu-sample-scale", type=int, default=21)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one untimed run on the device-resident graph (for profilers), then exit")

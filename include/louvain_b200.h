@@ -166,6 +166,17 @@ lv_status lv_community_create(lv_context* ctx, int64_t n, const int64_t* row_ptr
                               const int32_t* col, const float* w, int32_t in_mem,
                               lv_community** out);
 lv_status lv_community_destroy(lv_community* c);
+/* Resume a run checkpointed at the start of a level (no reference counterpart; the reference
+ * keeps nothing between levels but Community::best_communities and the contracted GraphDevice,
+ * community.h:16-26). A checkpoint is what the getters below return at a level start:
+ * lv_community_info (n0, level, weights_integer, and `iterations` = passes so far from
+ * lv_stats or the trace), lv_community_get_graph (the level's CSR, weights as doubles) and
+ * lv_community_get_best (each input vertex's vertex at this level). Host memory. The resumed
+ * run continues exactly as the interrupted one would (integer weights: bit-identical). */
+lv_status lv_community_resume(lv_context* ctx, int64_t n0, const int32_t* best, int32_t level,
+                              int32_t iterations, int64_t n, const int64_t* row_ptr,
+                              const int32_t* col, const double* w, int32_t weights_integer,
+                              lv_community** out);
 /* One OptimizationPhase::optimize() + Community::compute_modularity()
  * (phaseOptimization.cuh:116-155,171): returns Q_after - Q_before and the number of moves. */
 lv_status lv_optimization_step(lv_community* c, double* delta_q, int64_t* n_moved);

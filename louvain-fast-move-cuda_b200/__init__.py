@@ -98,7 +98,7 @@ TRACE_DTYPE = np.dtype([
 EXPORTS = (
     "lv_config_default", "lv_create", "lv_destroy", "lv_last_error", "lv_status_string",
     "lv_abi_version", "lv_run_csr", "lv_run_batch", "lv_autotune", "lv_community_create",
-    "lv_community_destroy", "lv_optimization_step", "lv_optimization_run",
+    "lv_community_destroy", "lv_community_resume", "lv_optimization_step", "lv_optimization_run",
     "lv_aggregation_run", "lv_louvain", "lv_community_info_get", "lv_community_get_partition",
     "lv_community_get_best", "lv_community_get_graph", "lv_community_get_trace",
     "lv_server_create", "lv_server_destroy", "lv_server_submit", "lv_server_submit_borrowed",
@@ -131,6 +131,7 @@ def load_library(path: Optional[str] = None):
         "lv_autotune": (i32, [vp, i32, vp, vp, vp, vp, i32, i32, P(Config), P(dbl)]),
         "lv_community_create": (i32, [vp, i64, vp, vp, vp, i32, P(vp)]),
         "lv_community_destroy": (i32, [vp]),
+        "lv_community_resume": (i32, [vp, i64, vp, i32, i32, i64, vp, vp, vp, i32, P(vp)]),
         "lv_optimization_step": (i32, [vp, P(dbl), P(i64)]),
         "lv_optimization_run": (i32, [vp, P(i32)]),
         "lv_aggregation_run": (i32, [vp, i32]),
@@ -298,6 +299,20 @@ class Engine:
         GPU with the reference's GraphHost rules (graph.cu:17-87)."""
         return Ingest(self, source, skip_line)
 
+    def resume(self, ckpt: dict) -> "CommunityState":
+        """lv_community_resume from CommunityState.checkpoint()'s dict."""
+        row = np.ascontiguousarray(ckpt["row_ptr"], dtype=np.int64)
+        col = np.ascontiguousarray(ckpt["col"], dtype=np.int32)
+        w = np.ascontiguousarray(ckpt["w"], dtype=np.float64)
+        best = np.ascontiguousarray(ckpt["best"], dtype=np.int32)
+        h = ctypes.c_void_p()
+        self.check(self._L.lv_community_resume(self._h, int(ckpt["n0"]), best.ctypes.data,
+                                               int(ckpt["level"]), int(ckpt["iterations"]),
+                                               row.size - 1, row.ctypes.data, col.ctypes.data,
+                                               w.ctypes.data, int(ckpt["weights_integer"]),
+                                               ctypes.byref(h)), "lv_community_resume")
+        return CommunityState(self, None, _handle=h, _n0=int(ckpt["n0"]))
+
     def community(self, g: CSRGraph) -> "CommunityState":
         return CommunityState(self, g)
 
@@ -306,8 +321,12 @@ class CommunityState:
     """Phase-level handle (lv_community): the reference's Community plus the phase calls
     OptimizationPhase::run / AggregationPhase::run that modularity_routine makes."""
 
-    def __init__(self, engine: Engine, g: CSRGraph):
+    def __init__(self, engine: Engine, g: Optional[CSRGraph], _handle=None, _n0: int = 0):
         self.e = engine
+        if _handle is not None:  # built by Engine.resume
+            self._h = _handle
+            self.n0 = _n0
+            return
         self._row = np.ascontiguousarray(g.row_ptr, dtype=np.int64)
         self._col = np.ascontiguousarray(g.col, dtype=np.int32)
         self._w = None if g.w is None else np.ascontiguousarray(g.w, dtype=np.float32)
@@ -325,6 +344,16 @@ class CommunityState:
 
     def __del__(self):
         self.close()
+
+    def checkpoint(self) -> dict:
+        """The run's state at a level start (call after aggregation_run(True), before the
+        next optimisation): enough for Engine.resume to continue it anywhere."""
+        info = self.info()
+        tr = self.trace()
+        row, col, w, _ = self.graph()
+        return {"n0": int(info.n0), "level": int(info.level), "iterations": int(len(tr)),
+                "weights_integer": int(info.weights_integer), "row_ptr": row, "col": col,
+                "w": np.asarray(w, dtype=np.float64), "best": self.best().astype(np.int32)}
 
     def optimization_step(self):
         d = ctypes.c_double(0)

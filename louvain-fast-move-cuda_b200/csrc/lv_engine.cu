@@ -409,6 +409,46 @@ class Run {
     const int32_t* col;
     const float* w;
   };
+  // The start of level `level` of a run that was checkpointed there: the level's CSR (weights as
+  // doubles: exact integers in integer mode, fp32 values otherwise), and for each of the n0
+  // input vertices its vertex at this level. Everything else a level start holds (k, m, the
+  // self-loop weight, the identity partition) follows from the CSR.
+  void init_resume(int64_t n0_, const int32_t* best, int32_t level, int32_t iterations, int64_t n_,
+                   const int64_t* row_ptr, const int32_t* col, const double* w, bool integer) {
+    if (n_ <= 0 || n0_ < n_ || !row_ptr || !col || !best || !w || level < 0 || iterations < 0)
+      throw Fail{LV_ERR_ARGUMENT, "resume: n0 >= n > 0, row_ptr, col, w and best are required"};
+    if (n0_ >= 0xFFFFFFFFll) throw Fail{LV_ERR_RANGE, "more than 2^32-2 vertices"};
+    const int64_t E64 = row_ptr[n_];
+    for (int64_t i = 0; i < n0_; ++i)
+      if (best[i] < 0 || best[i] >= n_) throw Fail{LV_ERR_INPUT, "resume: best[] outside the level's vertices"};
+    allocate(1, n_, E64, n0_);
+    if (integer) {
+      std::vector<uint32_t> wu((size_t)E);
+      for (size_t e = 0; e < wu.size(); ++e) {
+        const double x = w[e];
+        if (!(x >= 1.0) || x != std::floor(x) || x > 4294967295.0)
+          throw Fail{LV_ERR_INPUT, "resume: integer weights must be whole numbers in [1, 2^32)"};
+        wu[e] = (uint32_t)x;
+      }
+      LV_CUDA(cudaMemcpyAsync(D.wB, wu.data(), (size_t)E * 4, cudaMemcpyHostToDevice, st));
+    } else {
+      std::vector<float> wf((size_t)E);
+      for (size_t e = 0; e < wf.size(); ++e) wf[e] = (float)w[e];
+      LV_CUDA(cudaMemcpyAsync(D.w, wf.data(), (size_t)E * 4, cudaMemcpyHostToDevice, st));
+    }
+    set_weight_mode(integer);
+    LV_CUDA(cudaMemcpyAsync(D.col, col, (size_t)E * 4, cudaMemcpyHostToDevice, st));
+    LV_CUDA(cudaMemcpyAsync(row64(), row_ptr, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
+    const std::vector<int64_t> ho = {0, n_};
+    prepare(ho, nullptr, true, integer ? reinterpret_cast<const uint32_t*>(D.wB) : nullptr);
+    // the checkpoint's vertex map and counters replace the fresh run's
+    LV_CUDA(cudaMemcpyAsync(D.best, best, (size_t)n0 * 4, cudaMemcpyHostToDevice, st));
+    const uint32_t lv_it[2] = {(uint32_t)level, (uint32_t)iterations};
+    LV_CUDA(cudaMemcpyAsync(&D.gs[0].level, &lv_it[0], 4, cudaMemcpyHostToDevice, st));
+    LV_CUDA(cudaMemcpyAsync(&D.gs[0].total_iters, &lv_it[1], 4, cudaMemcpyHostToDevice, st));
+    sync();
+  }
+
   void init_pieces(const std::vector<Piece>& ps) {
     if (ps.empty()) throw Fail{LV_ERR_ARGUMENT, "empty batch"};
     std::vector<int64_t> ho(ps.size() + 1, 0), eo(ps.size() + 1, 0);
@@ -441,12 +481,13 @@ class Run {
  private:
   long long* row64() { return reinterpret_cast<long long*>(D.cd); }  // (n+1) x 8 B, free until aggregation
 
-  void allocate(uint32_t G_, int64_t n_, int64_t E64) {
+  void allocate(uint32_t G_, int64_t n_, int64_t E64, int64_t n0_ = -1) {
     if (E64 <= 0) throw Fail{LV_ERR_INPUT, "graph has no edges"};
     // hash tables are sized next_pow2(2 x row length) in u32 arithmetic
     if (E64 > (1ll << 30)) throw Fail{LV_ERR_RANGE, "more than 2^30 edge entries"};
     G = G_;
-    n0 = n = (uint32_t)n_;
+    n = (uint32_t)n_;
+    n0 = n0_ > 0 ? (uint32_t)n0_ : n;
     E = (uint32_t)E64;
     m_edges = E64 / 2;
     if (!pinned) {
@@ -507,7 +548,10 @@ class Run {
       sync();
       wm = pinned[0] ? LV_WEIGHTS_FLOAT : LV_WEIGHTS_INTEGER;
     }
-    wint = wm == LV_WEIGHTS_INTEGER;
+    set_weight_mode(wm == LV_WEIGHTS_INTEGER);
+  }
+  void set_weight_mode(bool integer) {
+    wint = integer;
     setup_bins();
     if (wint) configure_kernels<true>(); else configure_kernels<false>();
     grid_n = ctx->sms * 8;
@@ -515,7 +559,8 @@ class Run {
   }
 
   // Control block, graph states, graph ids, degrees and totals, then the first level.
-  void prepare(const std::vector<int64_t>& ho, const long long* doffs, bool weighted) {
+  void prepare(const std::vector<int64_t>& ho, const long long* doffs, bool weighted,
+               const uint32_t* wu = nullptr) {
     LV_CUDA(cudaMemsetAsync(D.ctrl, 0, sizeof(Ctrl), st));
     LV_CUDA(cudaMemsetAsync(D.gs, 0, sizeof(GraphState) * G, st));
     Ctrl hc{};
@@ -538,12 +583,12 @@ class Run {
       LV_CUDA(cudaMemcpyAsync(D.gid0, D.gid, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
       ++launches;
     }
-    const float* wf = weighted ? reinterpret_cast<const float*>(D.w) : nullptr;
+    const float* wf = weighted && !wu ? reinterpret_cast<const float*>(D.w) : nullptr;
     iota_best();
-    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, n, E);
-    else k_prep<false><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, n, E);
-    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf);
-    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf);
+    if (wint) k_prep<true><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, wu, n, E);
+    else k_prep<false><<<grid_n, 256, 0, st>>>(Dd, row64(), wf, wu, n, E);
+    if (wint) k_prep_long<true><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf, wu);
+    else k_prep_long<false><<<ctx->sms * 4, 512, 0, st>>>(Dd, wf, wu);
     if (wint) k_prep_total<true><<<1, 256, 0, st>>>(Dd);
     else k_prep_total<false><<<1, 256, 0, st>>>(Dd);
     launches += 4;
@@ -1163,6 +1208,22 @@ lv_status lv_community_create(lv_context* ctx, int64_t n, const int64_t* row_ptr
     c->ctx = ctx;
     c->run = std::make_unique<lv::Run>(ctx);
     c->run->init(1, nullptr, n, row_ptr, col, w, in_mem);
+    *out = c.release();
+  });
+}
+
+lv_status lv_community_resume(lv_context* ctx, int64_t n0, const int32_t* best, int32_t level,
+                              int32_t iterations, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                              const double* w, int32_t weights_integer, lv_community** out) {
+  if (!ctx || !out) return LV_ERR_ARGUMENT;
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->device);
+    auto c = std::make_unique<lv_community>();
+    c->ctx = ctx;
+    c->run = std::make_unique<lv::Run>(ctx);
+    c->run->init_resume(n0, best, level, iterations, n, row_ptr, col, w, weights_integer != 0);
     *out = c.release();
   });
 }

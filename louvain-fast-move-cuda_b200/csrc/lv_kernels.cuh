@@ -1159,15 +1159,19 @@ constexpr uint32_t kPrepLongRow = 4096;
 template <bool WINT>
 __device__ __forceinline__ void prep_entries(const Dev& D, uint32_t v, long long e0, long long re,
                                              uint32_t step, uint32_t lo, uint32_t hi, const float* wf_in,
-                                             unsigned long long& ki, unsigned long long& si,
-                                             double& kf, double& sf, uint32_t& err) {
+                                             const uint32_t* wu_in, unsigned long long& ki,
+                                             unsigned long long& si, double& kf, double& sf,
+                                             uint32_t& err) {
   for (long long e = e0; e < re; e += step) {
     const uint32_t u = D.col[e];
     if (u < lo || u >= hi) { err |= kErrInput; continue; }
     const float x = wf_in ? wf_in[e] : 1.0f;
     if (WINT) {
-      if (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f) { err |= kErrInput; continue; }
-      const uint32_t xi = (uint32_t)x;
+      // integer weights come as floats (exact below 2^24) or, for a resumed level whose sums
+      // may exceed that, as u32 (wu_in)
+      if (!wu_in && (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f)) { err |= kErrInput; continue; }
+      const uint32_t xi = wu_in ? wu_in[e] : (uint32_t)x;
+      if (xi == 0u) { err |= kErrInput; continue; }
       reinterpret_cast<uint32_t*>(D.w)[e] = xi;
       ki += xi;
       if (u == v) si += xi;
@@ -1182,6 +1186,7 @@ __device__ __forceinline__ void prep_entries(const Dev& D, uint32_t v, long long
 
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64, const float* wf_in,
+                                              const uint32_t* wu_in,
                                               uint32_t n, unsigned long long E) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
@@ -1227,7 +1232,7 @@ __global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64,
     }
     unsigned long long ki = 0, si = 0;
     double kf = 0.0, sf = 0.0;
-    prep_entries<WINT>(D, v, rs + lane, re, 32, lo, hi, wf_in, ki, si, kf, sf, err);
+    prep_entries<WINT>(D, v, rs + lane, re, 32, lo, hi, wf_in, wu_in, ki, si, kf, sf, err);
     if (WINT) {
       ki = warp_sum(ki);
       si = warp_sum(si);
@@ -1248,7 +1253,7 @@ __global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64,
 
 // Rows longer than kPrepLongRow entries, one block each.
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in) {
+__global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in, const uint32_t* wu_in) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   __shared__ unsigned long long shu[33];
@@ -1261,7 +1266,7 @@ __global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     unsigned long long ki = 0, si = 0;
     double kf = 0.0, sf = 0.0;
-    prep_entries<WINT>(D, v, rs + threadIdx.x, re, blockDim.x, D.gs[g].vb, D.gs[g].ve, wf_in, ki, si, kf, sf, err);
+    prep_entries<WINT>(D, v, rs + threadIdx.x, re, blockDim.x, D.gs[g].vb, D.gs[g].ve, wf_in, wu_in, ki, si, kf, sf, err);
     if (WINT) {
       ki = block_sum<512>(ki, shu);
       si = block_sum<512>(si, shu);
