@@ -368,9 +368,13 @@ def run_served(args, local):
     loop_gps = len(pool) / loop_s
 
     srv = lv.Server(eng, 150 << 30, slots=args.slots)
-    for g in pool[:args.slots]:
-        srv.submit(g, borrow=True)
-    srv.drain()
+    # warm-up: the whole pool twice in a burst, so that every slot captures its level loop and
+    # the memory pool holds every size before the timed rates
+    for _ in range(2):
+        ids = [srv.submit(g, borrow=True) for g in pool]
+        srv.drain()
+        for rid in ids:
+            srv.poll(rid)
     rates = []
     worst_dq = 0.0
     with ClockSampler(local) as clk:
