@@ -79,10 +79,19 @@ typedef struct {
                                captured CUDA graph with device-side loop control, captured once
                                per context (or serving slot) and replayed (default);
                                0 = host-driven, one stream launch sequence per pass */
-  int32_t reserved_i[7];
+  int32_t refine;           /* 1 = refine each level's partition before aggregating it (a
+                               Leiden-style refinement behind the reference's empty
+                               RefinePhase hook, phaseRefine.cuh:1-3; no reference
+                               counterpart). Host-driven runs only (use_graphs is ignored);
+                               not available to the server or lv_community_resume. Default 0 */
+  int32_t refine_passes;    /* refinement passes per level at most; 0 = until a pass raises the
+                               refined partition's modularity by no more than `threshold` */
+  int32_t reserved_i[5];
   /* degree-bin tiling; 0 = use the autotuned or built-in table */
   int32_t bin_max_degree[8];
-  double reserved_d[4];
+  double refine_tolerance;  /* a refined level also continues while its aggregate graph has
+                               fewer than refine_tolerance x n vertices (default 0.95) */
+  double reserved_d[3];
 } lv_config;
 
 /* Per-run statistics (modularityAlgorithms.h:18-20,73-79 "Metrics" line and more). */
@@ -111,7 +120,8 @@ typedef struct {
   int64_t active_vertices;      /* sum over passes of the active vertices */
   int64_t graph_launches;       /* launches of the captured level loop (0: host-driven run;
                                    more than 1 when the run stopped to grow its hash arena) */
-  int64_t reserved[2];
+  int64_t refine_passes;        /* refinement passes over all levels (refine = 1) */
+  int64_t reserved[1];
 } lv_stats;
 
 typedef struct lv_context lv_context;
@@ -119,7 +129,9 @@ typedef struct lv_community lv_community;
 
 /* ---- context --------------------------------------------------------------------------
  * A context owns one device, its streams and a reusable device arena (the reference
- * re-allocates 6 x STEP_ROUND scratch vectors on every level, phaseOptimization.cuh:50-68). */
+ * re-allocates 6 x STEP_ROUND scratch vectors on every level, phaseOptimization.cuh:50-68).
+ * Communities, ingested graphs and servers created on a context use it until they are
+ * destroyed: destroy them before the context. */
 void lv_config_default(lv_config* cfg);
 lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out);
 lv_status lv_destroy(lv_context* ctx);

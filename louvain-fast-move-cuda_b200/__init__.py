@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes
 import enum
 import os
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
@@ -54,8 +55,10 @@ class Config(ctypes.Structure):
         ("max_iterations", ctypes.c_int32), ("max_levels", ctypes.c_int32),
         ("threshold", ctypes.c_double), ("chunk_edges", ctypes.c_int64),
         ("weight_mode", ctypes.c_int32), ("validate", ctypes.c_int32),
-        ("use_graphs", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 7),
-        ("bin_max_degree", ctypes.c_int32 * 8), ("reserved_d", ctypes.c_double * 4),
+        ("use_graphs", ctypes.c_int32), ("refine", ctypes.c_int32),
+        ("refine_passes", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 5),
+        ("bin_max_degree", ctypes.c_int32 * 8), ("refine_tolerance", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 3),
     ]
 
 
@@ -70,7 +73,8 @@ class Stats(ctypes.Structure):
         ("bytes_optimization", ctypes.c_double), ("ms_optimization_kernels", ctypes.c_float),
         ("reserved1", ctypes.c_int32), ("kernel_launches", ctypes.c_int64),
         ("active_entries", ctypes.c_int64), ("active_vertices", ctypes.c_int64),
-        ("graph_launches", ctypes.c_int64), ("reserved", ctypes.c_int64 * 2),
+        ("graph_launches", ctypes.c_int64), ("refine_passes", ctypes.c_int64),
+        ("reserved", ctypes.c_int64 * 1),
     ]
 
     def as_dict(self) -> dict:
@@ -184,7 +188,9 @@ def _is_device(a) -> bool:
 def config(mode: int = MODE.SORT, threshold: float = 1e-3, fast_first: bool = True,
            chunk_edges: int = 50_000_000, max_iterations: int = 1_000_000_000,
            max_levels: int = 0, weight_mode: int = WEIGHTS_AUTO,
-           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = True) -> Config:
+           bin_max_degree: Optional[Sequence[int]] = None, use_graphs: bool = True,
+           refine: bool = False, refine_passes: int = 0,
+           refine_tolerance: Optional[float] = None) -> Config:
     c = Config()
     load_library().lv_config_default(ctypes.byref(c))
     c.mode = int(mode)
@@ -195,6 +201,10 @@ def config(mode: int = MODE.SORT, threshold: float = 1e-3, fast_first: bool = Tr
     c.max_levels = int(max_levels)
     c.weight_mode = int(weight_mode)
     c.use_graphs = int(bool(use_graphs))
+    c.refine = int(bool(refine))
+    c.refine_passes = int(refine_passes)
+    if refine_tolerance is not None:
+        c.refine_tolerance = float(refine_tolerance)
     if bin_max_degree is not None:
         for i, d in enumerate(bin_max_degree[:8]):
             c.bin_max_degree[i] = int(d)
@@ -206,6 +216,7 @@ class Engine:
 
     def __init__(self, device: int = 0, cfg: Optional[Config] = None, **kw):
         self._L = load_library()
+        self._deps = weakref.WeakSet()
         self.cfg = cfg if cfg is not None else config(**kw)
         h = ctypes.c_void_p()
         st = self._L.lv_create(int(device), ctypes.byref(self.cfg), ctypes.byref(h))
@@ -215,6 +226,9 @@ class Engine:
 
     def close(self):
         if getattr(self, "_h", None):
+            # communities, ingested graphs and servers use the context: they go first
+            for d in list(getattr(self, "_deps", ())):
+                d.close()
             self._L.lv_destroy(self._h)
             self._h = None
 
@@ -326,6 +340,7 @@ class CommunityState:
         if _handle is not None:  # built by Engine.resume
             self._h = _handle
             self.n0 = _n0
+            engine._deps.add(self)
             return
         self._row = np.ascontiguousarray(g.row_ptr, dtype=np.int64)
         self._col = np.ascontiguousarray(g.col, dtype=np.int32)
@@ -336,11 +351,13 @@ class CommunityState:
         engine.check(st, "lv_community_create")
         self._h = h
         self.n0 = g.n
+        engine._deps.add(self)
 
     def close(self):
-        if getattr(self, "_h", None):
+        # (a context already destroyed took this object's device memory with it)
+        if getattr(self, "_h", None) and getattr(self.e, "_h", None):
             self.e._L.lv_community_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
@@ -434,14 +451,15 @@ class Ingest:
         engine.check(engine._L.lv_ingest_edge_list(engine._h, ptr, size, int(skip_line), MEM_HOST,
                                                    ctypes.byref(h)), "lv_ingest_edge_list")
         self._h = h
+        engine._deps.add(self)
         n, m, E, mn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         engine._L.lv_ingest_info(h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(E), ctypes.byref(mn))
         self.n_nodes, self.n_links, self.entries, self.min_id = n.value, m.value, E.value, mn.value
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self.e, "_h", None):
             self.e._L.lv_ingest_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
@@ -475,12 +493,13 @@ class Server:
         self._h = h
         self.n_of = {}
         self._held = {}
+        engine._deps.add(self)
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self.e, "_h", None):
             self.e._L.lv_server_destroy(self._h)  # joins the workers: borrowed buffers are free after
-            self._h = None
-            self._held = {}
+        self._h = None
+        self._held = {}
 
     def __del__(self):
         self.close()

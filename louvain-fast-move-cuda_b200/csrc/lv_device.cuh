@@ -3,25 +3,10 @@
 // reductions and scans.
 #pragma once
 
-#include <cooperative_groups.h>
-#include <cooperative_groups/reduce.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace lv {
-
-namespace cg = cooperative_groups;
-
-// Warp aggregation of a keyed update: the active lanes holding the same key add their values
-// together and one of them passes (key, sum) to `sink`. Turns up to 32 atomics on one hot
-// address into one. Callable from divergent code.
-template <class K, class V, class F>
-__device__ __forceinline__ void warp_combine(K key, V val, F&& sink) {
-  const cg::coalesced_group act = cg::coalesced_threads();
-  const auto grp = cg::labeled_partition(act, key);
-  const V sum = cg::reduce(grp, val, cg::plus<V>());
-  if (grp.thread_rank() == 0) sink(key, sum);
-}
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;  // empty hash slot / no community
 constexpr uint32_t kNever = 0xFFFFFFFFu;  // iteration stamp that never matches

@@ -24,6 +24,7 @@
 
 #include "../../include/louvain_b200.h"
 #include "lv_kernels.cuh"
+#include "lv_refine.cuh"
 
 namespace lv {
 
@@ -87,7 +88,8 @@ struct DevSlot {
 // A context keeps the device memory of finished runs in a pool and hands it to the next run,
 // so repeated calls allocate nothing (cudaMalloc / cudaFree synchronise the whole device).
 struct lv_context {
-  lv::DevSlot slot;  // the Dev buffer and captured graph of runs on `stream`
+  lv::DevSlot slot;   // the Dev buffer and captured graph of runs on `stream`
+  lv::DevSlot rslot;  // the refine view's Dev (claimed by the first refining run)
   int device = 0;
   lv_config cfg{};
   int sms = 148;
@@ -261,7 +263,7 @@ class Run {
   // used the slot in between). Stream-ordered, so kernels launched afterwards see it.
   void bind() {
     if (slot->owner == this && !dev_dirty) return;
-    LV_CUDA(cudaMemcpyToSymbolAsync(c_dev, &D, sizeof(Dev), (size_t)Dd * sizeof(Dev),
+    LV_CUDA(cudaMemcpyToSymbolAsync(c_dev, &D, sizeof(Dev), (size_t)slot->id * sizeof(Dev),
                                     cudaMemcpyHostToDevice, st));
     slot->owner = this;
     dev_dirty = false;
@@ -531,6 +533,17 @@ class Run {
       D.gid0 = dalloc<uint32_t>(ctx, owned, n0);
     }
     D.scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2);
+    if (cfg.refine) {
+      D.ref = dalloc<uint32_t>(ctx, owned, n);
+      D.ref_new = dalloc<uint32_t>(ctx, owned, n);
+      D.aref = dalloc<double>(ctx, owned, n);
+      D.rsz = dalloc<uint32_t>(ctx, owned, n);
+      D.rflag = dalloc<uint32_t>(ctx, owned, n);
+      D.gsR = dalloc<GraphState>(ctx, owned, G);
+      D.coarse = dalloc<uint32_t>(ctx, owned, n);
+      D.lab = dalloc<uint32_t>(ctx, owned, n);
+      D.prev = dalloc<uint32_t>(ctx, owned, n);
+    }
     dev_dirty = true;
     bind();
   }
@@ -615,9 +628,11 @@ class Run {
     if (wint) k_commit_sq<true><<<grid_sq, 256, 0, st>>>(Dd, single() ? 1 : 0);
     else k_commit_sq<false><<<grid_sq, 256, 0, st>>>(Dd, single() ? 1 : 0);
   }
-  void finalize(int level_start_flag) {
-    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
-    else k_finalize<false><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, cfg.fast_first, gc);
+  // view: a refinement pass (regular passes only: no fast pass, no trace record)
+  void finalize(int level_start_flag, bool view = false) {
+    const int ff = view ? 0 : cfg.fast_first, vw = view ? 1 : 0;
+    if (wint) k_finalize<true><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, ff, gc, vw);
+    else k_finalize<false><<<1, 1024, 0, st>>>(Dd, single() ? 1 : 0, grid_sq, level_start_flag, cfg.mode, ff, gc, vw);
   }
 
   void ensure_arena(uint64_t need_slots) {
@@ -649,7 +664,8 @@ class Run {
     }
     k_level_init<<<grid_n, 256, 0, st>>>(Dd);
     commit_sq();
-    finalize(1);
+    // a refined run measures a level's gain from the previous level's end (k_ref_decide)
+    finalize(cfg.refine && levels_run > 0 ? 2 : 1);
     k_arena_need<<<grid_n, 256, 0, st>>>(Dd, bins.maxdeg[6], bins.block_cap);
     launches += 4;
   }
@@ -661,7 +677,7 @@ class Run {
 
   // ---- one optimisation pass --------------------------------------------------------------------
   template <bool WI>
-  void launch_pass() {
+  void launch_pass(bool view = false) {
     const size_t slot = 4 + (WI ? 4 : 8);
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
     k_chunk_flags<<<grid_n, 256, 0, st>>>(Dd);
@@ -678,12 +694,17 @@ class Run {
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(Dd);
+    if (view) {
+      k_ref_resolve<<<grid_n, 256, 0, st>>>(Dd);
+      k_ref_reject<<<grid_n, 256, 0, st>>>(Dd);
+      launches += 2;
+    }
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[5], st));
     k_apply<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_long<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
     commit_sq();
-    finalize(0);
+    finalize(0, view);
     launches += 18;
   }
 
@@ -715,14 +736,81 @@ class Run {
   // the arena check and let the host redo the aggregation with a larger arena.
   template <bool WI>
   void agg_prefix(int force) {
+    agg_decide(force, 0);
+    agg_renumber<WI>();
+  }
+  void agg_decide(int force, int defer_i) {
     const uint32_t gb = 32;  // grid-stride over graphs; fixed so that captured graphs are reusable
-    k_agg_decide<<<gb, 256, 0, st>>>(Dd, force, (uint32_t)std::max(0, cfg.max_levels));
+    k_agg_decide<<<gb, 256, 0, st>>>(Dd, force, (uint32_t)std::max(0, cfg.max_levels), defer_i);
+    ++launches;
+  }
+  template <bool WI>
+  void agg_renumber() {
+    const uint32_t gb = 32;
     k_agg_clear_map<<<grid_n, 256, 0, st>>>(Dd);
     k_agg_mark<<<grid_n, 256, 0, st>>>(Dd);
     k_agg_flags<<<grid_n, 256, 0, st>>>(Dd);
     scan<unsigned long long, true, kScanMap>();
     k_agg_meta<<<gb, 256, 0, st>>>(Dd);
-    launches += 5;
+    launches += 4;
+  }
+
+  // ---- refinement (lv_refine.cuh) -------------------------------------------------------------
+  // Between the level's decision and its renumbering: restricted rows, refinement passes in
+  // the refine view, then the per-graph decision and the swap to the refined partition.
+  int Dr = -1;  // the refine view's c_dev slot
+  int64_t refine_passes_run = 0;
+  void bind_refine() {
+    if (ctx->rslot.id < 0 && ctx->rslot.create() != cudaSuccess)
+      throw Fail{LV_ERR_CUDA, "no free device slot for the refine view"};
+    Dr = ctx->rslot.id;
+    Dev R = D;
+    R.row = D.rowB;
+    R.col = D.colB;
+    R.w = D.wB;
+    R.comm = D.ref;
+    R.new_comm = D.ref_new;
+    R.a = D.aref;
+    R.gs = D.gsR;
+    LV_CUDA(cudaMemcpyToSymbolAsync(c_dev, &R, sizeof(Dev), (size_t)Dr * sizeof(Dev),
+                                    cudaMemcpyHostToDevice, st));
+  }
+  template <bool WI>
+  void refine(int force) {
+    const uint32_t ml = (uint32_t)std::max(0, cfg.max_levels);
+    k_ref_init<<<grid_n, 256, 0, st>>>(Dd, ml);
+    k_ref_count<WI><<<grid_n, 256, 0, st>>>(Dd);
+    scan<uint32_t, false, kScanDeg>();
+    k_ref_fill<WI><<<grid_n, 256, 0, st>>>(Dd);
+    launches += 3;
+    // The restricted rows are no longer than the level's rows, so the level start's arena
+    // already holds every global table a refinement pass can need.
+    bind_refine();
+    const int main = Dd;
+    Dd = Dr;
+    try {
+      commit_sq();
+      finalize(1, true);
+      launches += 2;
+      for (int64_t p = 0;; ++p) {
+        const uint32_t left = ctrl_u32(offsetof(Ctrl, n_iterating));
+        if (left == 0 || (cfg.refine_passes > 0 && p >= cfg.refine_passes)) break;
+        if (p >= (int64_t)kGuardPasses) throw Fail{LV_ERR_DEVICE_CHECK, "refinement passes beyond their guard"};
+        k_ref_select<<<grid_n, 256, 0, st>>>(Dd);
+        ++launches;
+        launch_pass<WI>(true);
+        ++refine_passes_run;
+      }
+    } catch (...) {
+      Dd = main;
+      throw;
+    }
+    Dd = main;
+    k_ref_labels<<<grid_n, 256, 0, st>>>(Dd);
+    k_ref_decide<<<32, 256, 0, st>>>(Dd, force, cfg.refine_tolerance);
+    k_ref_swap<<<grid_n, 256, 0, st>>>(Dd);
+    launches += 3;
+    check_device_errors();
   }
   template <bool WI>
   void agg_contract_a() {
@@ -763,10 +851,28 @@ class Run {
   // Returns true if any graph continues to a new level.
   template <bool WI>
   bool aggregate_impl(int force) {
-    agg_prefix<WI>(force);
+    if (cfg.refine) {
+      agg_decide(force, 1);
+      // every iterating graph is at level levels_run: none refines at the level cap
+      const bool at_cap = cfg.max_levels > 0 && levels_run + 1 >= cfg.max_levels;
+      if (force != 0 && !at_cap) refine<WI>(force);
+      if (force < 0 && levels_run > 0) {
+        k_ref_revert_comm<<<grid_n, 256, 0, st>>>(Dd);
+        k_ref_revert_q<<<32, 256, 0, st>>>(Dd);
+        launches += 2;
+      }
+      agg_renumber<WI>();
+    } else {
+      agg_prefix<WI>(force);
+    }
     const uint32_t n2 = ctrl_u32(offsetof(Ctrl, n_next));
     if (n2 > 0) {
       agg_contract_a<WI>();
+      if (cfg.refine) {
+        k_ref_prev_label<<<grid_n, 256, 0, st>>>(Dd);
+        k_ref_prev<<<grid_n, 256, 0, st>>>(Dd);
+        launches += 2;
+      }
       const uint32_t need = ctrl_u32(offsetof(Ctrl, hub_cursor));
       if (debug) {
         uint32_t bc[kNumBins];
@@ -1041,7 +1147,7 @@ class Run {
 
   // modularity_routine's level loop: captured and device-driven (use_graphs), or host-driven.
   void louvain() {
-    if (cfg.use_graphs && !debug && !finished) {
+    if (cfg.use_graphs && !cfg.refine && !debug && !finished) {
       if (wint) louvain_graph<true>(); else louvain_graph<false>();
       return;
     }
@@ -1084,6 +1190,7 @@ class Run {
       s->levels = (int32_t)seg_counts().levels;
     }
     s->graph_launches = graph_launches;
+    s->refine_passes = refine_passes_run;
     s->iterations = (int32_t)hs[0].total_iters;
     s->n_communities = (int32_t)hs[0].n_best;
     s->ms_optimization = (float)t_opt_ms;
@@ -1151,6 +1258,9 @@ void lv_config_default(lv_config* c) {
   c->weight_mode = LV_WEIGHTS_AUTO;
   c->validate = 1;
   c->use_graphs = 1;
+  c->refine = 0;
+  c->refine_passes = 0;
+  c->refine_tolerance = 0.95;
 }
 
 lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
@@ -1161,7 +1271,9 @@ lv_status lv_create(int32_t device, const lv_config* cfg, lv_context** out) {
   if (cfg) ctx->cfg = *cfg; else lv_config_default(&ctx->cfg);
   if (ctx->cfg.mode < 0 || ctx->cfg.mode > 3 || !(ctx->cfg.threshold >= 0) ||
       ctx->cfg.max_iterations < 0 || ctx->cfg.max_levels < 0 || ctx->cfg.chunk_edges < 0 ||
-      ctx->cfg.weight_mode < 0 || ctx->cfg.weight_mode > 2) {
+      ctx->cfg.weight_mode < 0 || ctx->cfg.weight_mode > 2 || ctx->cfg.refine < 0 ||
+      ctx->cfg.refine > 1 || ctx->cfg.refine_passes < 0 ||
+      !(ctx->cfg.refine_tolerance >= 0.0 && ctx->cfg.refine_tolerance <= 1.0)) {
     delete ctx;
     return LV_ERR_ARGUMENT;
   }
@@ -1186,6 +1298,7 @@ lv_status lv_destroy(lv_context* ctx) {
   if (!ctx) return LV_ERR_ARGUMENT;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->slot.destroy();
+  ctx->rslot.destroy();
   ctx->drain_pool();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto& ev : ctx->ev)
@@ -1219,6 +1332,9 @@ lv_status lv_community_resume(lv_context* ctx, int64_t n0, const int32_t* best, 
   *out = nullptr;
   std::lock_guard<std::mutex> lk(ctx->mu);
   return guarded(ctx, [&] {
+    // a refined run's level start also carries the previous level's end modularity, which
+    // the checkpoint does not hold
+    if (ctx->cfg.refine) throw Fail{LV_ERR_ARGUMENT, "resume of a refining configuration is not supported"};
     cudaSetDevice(ctx->device);
     auto c = std::make_unique<lv_community>();
     c->ctx = ctx;

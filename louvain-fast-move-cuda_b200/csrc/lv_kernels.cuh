@@ -56,6 +56,16 @@ struct Dev {
   uint32_t* gid0;            // [n0] graph of each input vertex (nullptr: one graph)
   int32_t* out;              // [n0] final community ids
   unsigned long long* scan_tmp;  // [(n + 1) / kScanTile + 2] tile sums of the scans
+  // refinement (allocated only when it is on; lv_refine.cuh)
+  uint32_t* ref;             // [n] refined partition
+  uint32_t* ref_new;         // [n] its pass targets
+  double* aref;              // [n] refined totals
+  uint32_t* rsz;             // [n] members per refined label
+  uint32_t* rflag;           // [n] kRefEligible / kRefReject
+  GraphState* gsR;           // [G] graph states of the refinement passes
+  uint32_t* coarse;          // [n] the level's partition, kept when aggregating by ref
+  uint32_t* lab;             // [n] per community of the level: its smallest next-level vertex
+  uint32_t* prev;            // [n] per vertex: its members' community at the previous level's end
 };
 
 // The Dev of every live slot (a context's, each serving slot's), in constant memory: kernels
@@ -765,11 +775,14 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
       v = D.movers[idx];
       old = D.comm[v];
       nw = D.new_comm[v];
-      rs = D.row[v];
-      len = D.row[v + 1] - rs;
-      const double kv = D.k[v];
-      atomicAdd(&D.a[nw], kv);
-      atomicAdd(&D.a[old], -kv);
+      // a refinement pass leaves rejected proposals in the list with new_comm == comm
+      if (nw != old) {
+        rs = D.row[v];
+        len = D.row[v + 1] - rs;
+        const double kv = D.k[v];
+        atomicAdd(&D.a[nw], kv);
+        atomicAdd(&D.a[old], -kv);
+      }
     }
     // long rows: queued for k_apply_long (the list lives in `members`, unused during passes)
     const bool defer = len > kApplyShort;
@@ -884,6 +897,7 @@ __global__ void __launch_bounds__(512) k_apply_hub(int dslot) {
     const unsigned long long item = D.apply_items[idx];
     const uint32_t v = (uint32_t)(item >> 32), piece = (uint32_t)item;
     const uint32_t old = D.comm[v], nw = D.new_comm[v];
+    if (nw == old) continue;  // a rejected refinement proposal (the whole block skips it)
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     if (threadIdx.x == 0 && piece == 0) {
       const double kv = D.k[v];
@@ -993,9 +1007,11 @@ __global__ void k_set_pass(Ctrl* C, uint32_t p, int mode, int fast_first) {
 // phaseOptimization.cuh:167-179: dQ = Q_after - Q_before; the level's passes stop when
 // dQ <= threshold (or after EARLY_STOP_LIMIT passes). `level_start` = 1 evaluates the level's
 // starting modularity instead (Community::update -> compute_modularity, community.h:57-65).
+// level_start = 2 keeps Q_level (a refined run's next level measures its gain from the
+// previous level's end). view = 1: a refinement pass (no trace record, no pass statistics).
 template <bool WINT>
 __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int nparts, int level_start,
-                                                   int mode, int fast_first, GraphCtl gc) {
+                                                   int mode, int fast_first, GraphCtl gc, int view) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   __shared__ double shd[33];
@@ -1028,7 +1044,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
     const double Q = modularity_of(I, S, st->m);
     if (level_start) {
       st->Q = Q;
-      st->Q_level = Q;
+      if (level_start == 1) st->Q_level = Q;
       st->iters = 0;
       ++iterating;
       continue;
@@ -1037,7 +1053,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
     st->Q = Q;
     st->iters += 1;
     st->total_iters += 1;
-    if (single) {
+    if (single && !view) {
       st->moved = C->mover_count + C->hub_mover_count;
       const uint32_t t = C->trace_len;
       if (t < kTraceCap) {
@@ -1065,8 +1081,10 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
     C->apply_items = 0;
     C->hub_cursor = 0;
     for (uint32_t i = 0; i < C->n_chunks && i < kMaxChunks; ++i) C->chunk_any[i] = 0;
-    C->act_entries_total += C->act_entries;
-    C->act_vertices_total += C->act_vertices;
+    if (!view) {
+      C->act_entries_total += C->act_entries;
+      C->act_vertices_total += C->act_vertices;
+    }
     C->act_entries = 0;
     C->act_vertices = 0;
     if (level_start) {
@@ -1074,8 +1092,10 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
     } else {
       C->it += 1;
       C->pass += 1;
-      C->seg_passes += 1;
-      C->t_opt_ns += global_ns() - C->t_pass0;
+      if (!view) {
+        C->seg_passes += 1;
+        C->t_opt_ns += global_ns() - C->t_pass0;
+      }
       if (C->seg_passes > kGuardPasses) atomicOr(&C->err, kErrLoop);
       // the captured pass loop runs while a graph iterates (and no guard has tripped)
       set_cond(gc, gc.pass, tot > 0 && !(C->err & kErrLoop));
@@ -2100,7 +2120,8 @@ __global__ void k_agg_finish(int dslot) {
 
 // Which graphs aggregate now and whether they continue: modularityAlgorithms.h:52
 // cont = Q_end - Q_level_start > threshold. force >= 0 overrides (phase-level API).
-__global__ void k_agg_decide(int dslot, int force, uint32_t max_levels) {
+// defer_i: a refined run resets I in k_ref_decide, once refinement has decided.
+__global__ void k_agg_decide(int dslot, int force, uint32_t max_levels, int defer_i) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -2116,7 +2137,7 @@ __global__ void k_agg_decide(int dslot, int force, uint32_t max_levels) {
     else cont = __dsub_rn(st->Q, st->Q_level) > C->threshold ? 1u : 0u;
     if (max_levels > 0 && st->level + 1 >= max_levels) cont = 0;
     st->cont = cont;
-    if (cont) st->I = 0;  // the contraction adds the next level's self-loop weight
+    if (cont && !defer_i) st->I = 0;  // the contraction adds the next level's self-loop weight
   }
 }
 

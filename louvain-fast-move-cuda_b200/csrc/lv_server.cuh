@@ -182,6 +182,11 @@ extern "C" {
 lv_status lv_server_create(lv_context* ctx, int64_t budget_bytes, int32_t max_slots, lv_server** out) {
   if (!ctx || !out || budget_bytes <= 0 || max_slots <= 0 || max_slots > 64) return LV_ERR_ARGUMENT;
   *out = nullptr;
+  // the serving slots run concurrently and the refine view has one device slot per context
+  if (ctx->cfg.refine) {
+    ctx->err = "the server does not run refining configurations";
+    return LV_ERR_ARGUMENT;
+  }
   auto s = std::make_unique<lv_server>();
   s->ctx = ctx;
   s->budget = budget_bytes;

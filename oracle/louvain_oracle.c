@@ -35,6 +35,33 @@
  *                                 best[v0] = new(comm[best[v0]]), contraction to sorted
  *                                 (c_s, c_d, sum w) rows, k' = row sums, identity restart
  *
+ * Refinement (cfg.refine = 1; no reference counterpart -- RefinePhase, phaseRefine.cuh:1-3, is
+ * an empty hook). The refinement step of Leiden (Traag, Waltman, van Eck 2019, "From Louvain to
+ * Leiden", Algorithm A.2 RefinePartition / MergeNodesSubset) in a greedy, pass-synchronous
+ * form, run after a level's local moving:
+ *   - the refined partition starts as singletons (ref[v] = v, aref[v] = k_v);
+ *   - v may move iff it is still a singleton and was well connected to its community S at the
+ *     start: 2m * w(v, S - v) >= k_v (K_S - k_v), K_S = a[S] (exact in 128-bit integers);
+ *   - a pass evaluates, for every such v, the refined communities of its neighbours inside S
+ *     with the gain and tie rule of a regular pass of the level's mode (own singleton:
+ *     self = 0, a_own = k_v) and proposes the best one if its gain is > 0;
+ *   - proposals are resolved from the pre-pass state: v -> t is kept unless t is a singleton
+ *     that itself proposes, except that of two singletons proposing each other the higher id
+ *     joins the lower; kept moves update ref, aref and the member counts;
+ *   - passes repeat while the refined partition's modularity rises by more than the threshold
+ *     (at most refine_passes passes when that is > 0, and the iteration limit).
+ * The level is then aggregated by the refined partition, and the next level starts from
+ * singletons as usual (Leiden starts it from the coarse partition; with the reference's
+ * synchronous moves that start oscillates, because the pass-0 v <= c gate only breaks the
+ * symmetry of a singleton start). A refined level continues iff its aggregate graph is
+ * smaller (n_ref < n) and either Q rose by more than the threshold since the previous
+ * level's end or n_ref < refine_tolerance * n; otherwise the run ends with the coarse
+ * partition -- or, when that level ended below the previous level's end, with the previous
+ * level's partition (each vertex of a level keeps its members' community of the level before,
+ * `prev`), so a refined run never ends below an earlier level's end. Refined communities are
+ * connected: a vertex only joins a community holding one of its neighbours that stays where
+ * it is.
+ *
  * Arithmetic: compiled with -ffp-contract=off so every double operation rounds once, as
  * the device code does. Weight sums are accumulated in double; with integer weights and
  * total weight below 2^32 (the reference's own u32 limit) every sum is exact, so summation
@@ -67,6 +94,9 @@ typedef struct {
     int64_t chunk_edges;     /* STEP_ROUND (constants.h:18); 0 disables the emulation */
     int32_t nthreads;        /* 0 = OpenMP default */
     int32_t integer_weights; /* 1 = weights are integers (reference semantics) */
+    int32_t refine;          /* 1 = refine the partition before each aggregation */
+    int32_t refine_passes;   /* refinement pass limit, 0 = until converged */
+    double refine_tolerance; /* a refined level continues while n_ref < tolerance * n */
 } orc_config;
 
 typedef struct {
@@ -100,6 +130,9 @@ typedef struct {
     int64_t n_best;
     int32_t level;
     int32_t iter_in_level;
+    int64_t refine_passes_run;
+    int32_t* prev;  /* refined runs: each vertex's community at the end of the previous level,
+                       labelled by the smallest vertex id of that community */
     /* scratch */
     int32_t* dec_c;
     float* dec_g;
@@ -222,7 +255,7 @@ void orc_destroy(orc_state* s) {
     if (!s) return;
     free_graph(s);
     free(s->comm); free(s->a); free(s->active); free(s->moved); free(s->best);
-    free(s->dec_c); free(s->dec_g); free(s->trace);
+    free(s->dec_c); free(s->dec_g); free(s->trace); free(s->prev);
     free(s);
 }
 
@@ -452,6 +485,145 @@ static int64_t optimization_step(orc_state* s) {
     return moved;
 }
 
+/* Modularity of an arbitrary partition `part` with totals `tot` (same arithmetic as
+ * compute_modularity). */
+static double partition_modularity(const orc_state* s, const int32_t* part, const double* tot) {
+    int64_t n = s->n;
+    double internal = 0.0, sq_d = 0.0;
+    if (s->cfg.integer_weights) {
+        uint64_t in = 0;
+        for (int64_t v = 0; v < n; v++)
+            for (int64_t e = s->row_ptr[v]; e < s->row_ptr[v + 1]; e++)
+                if (part[s->col[e]] == part[v]) in += s->wi[e];
+        unsigned __int128 sq = 0;
+        for (int64_t c = 0; c < n; c++) {
+            uint64_t ac = (uint64_t)tot[c];
+            sq += (unsigned __int128)ac * ac;
+        }
+        internal = (double)in;
+        sq_d = (double)sq;
+    } else {
+        for (int64_t v = 0; v < n; v++)
+            for (int64_t e = s->row_ptr[v]; e < s->row_ptr[v + 1]; e++)
+                if (part[s->col[e]] == part[v]) internal += s->wf[e];
+        for (int64_t c = 0; c < n; c++) sq_d += tot[c] * tot[c];
+    }
+    double m = s->m;
+    return internal / (2.0 * m) - sq_d / ((4.0 * m) * m);
+}
+
+/* The refinement of the current (coarse) partition s->comm; returns the refined partition
+ * (labels are vertex ids) or NULL when out of memory. Semantics in the header comment. */
+static int32_t* refine_partition(orc_state* s) {
+    int64_t n = s->n;
+    int32_t* ref = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+    int32_t* prop = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+    int32_t* rsz = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+    double* aref = (double*)malloc((size_t)n * sizeof(double));
+    uint8_t* wc = (uint8_t*)malloc((size_t)n);
+    uint8_t* keep = (uint8_t*)malloc((size_t)n);
+    if (!ref || !prop || !rsz || !aref || !wc || !keep) {
+        free(ref); free(prop); free(rsz); free(aref); free(wc); free(keep);
+        return NULL;
+    }
+    const double two_m = 2.0 * s->m;
+    for (int64_t v = 0; v < n; v++) {
+        const int32_t cv = s->comm[v];
+        if (s->cfg.integer_weights) {
+            uint64_t wv = 0;
+            for (int64_t e = s->row_ptr[v]; e < s->row_ptr[v + 1]; e++) {
+                int32_t u = s->col[e];
+                if (u != v && s->comm[u] == cv) wv += s->wi[e];
+            }
+            const uint64_t kv = (uint64_t)s->k[v], K = (uint64_t)s->a[cv];
+            wc[v] = (unsigned __int128)(uint64_t)two_m * wv >= (unsigned __int128)kv * (K - kv);
+        } else {
+            double wv = 0.0;
+            for (int64_t e = s->row_ptr[v]; e < s->row_ptr[v + 1]; e++) {
+                int32_t u = s->col[e];
+                if (u != v && s->comm[u] == cv) wv += s->wf[e];
+            }
+            wc[v] = two_m * wv >= s->k[v] * (s->a[cv] - s->k[v]);
+        }
+        ref[v] = (int32_t)v;
+        aref[v] = s->k[v];
+        rsz[v] = 1;
+    }
+    double q = partition_modularity(s, ref, aref);
+    const int m_ = s->cfg.mode;
+    for (int32_t p = 0;;) {
+        /* the level's tie rule for a regular pass with index p (phaseOptimization.cuh:135) */
+        const int hash_rule = m_ == 0 || m_ == 3 || (m_ == 2 && p > 4);
+        int nts = nthreads_for_scratch(s, n);
+        #pragma omp parallel num_threads(nts)
+        {
+            double* acc = (double*)malloc((size_t)n * sizeof(double));
+            int32_t* stamp = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+            int32_t* touched = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+            for (int64_t i = 0; i < n; i++) stamp[i] = -1;
+            #pragma omp for schedule(dynamic, 256)
+            for (int64_t v = 0; v < n; v++) {
+                prop[v] = ref[v];
+                if (!(ref[v] == (int32_t)v && rsz[v] == 1 && wc[v])) continue;
+                const int32_t cv = s->comm[v];
+                int32_t nt_ = 0;
+                for (int64_t e = s->row_ptr[v]; e < s->row_ptr[v + 1]; e++) {
+                    int32_t u = s->col[e];
+                    if (u == v || s->comm[u] != cv) continue;
+                    int32_t r = ref[u];
+                    if (stamp[r] != (int32_t)v) { stamp[r] = (int32_t)v; acc[r] = 0.0; touched[nt_++] = r; }
+                    acc[r] += wget(s, e);
+                }
+                if (nt_ == 0) continue;
+                sort_i32(touched, nt_);
+                const int32_t own = ref[v];
+                float self_v = (stamp[own] == (int32_t)v) ? (float)acc[own] : 0.0f;
+                double kv = s->k[v], a_own = aref[own];
+                int32_t bc = -1; float bg = 0.0f; int have = 0;
+                for (int32_t i = 0; i < nt_; i++) {
+                    int32_t c = touched[i];
+                    if (hash_rule && c == own) continue;
+                    float g = gain_ref((float)acc[c], self_v, kv, a_own, aref[c], s->m);
+                    if (hash_rule) {
+                        if (g > 0.0f && (!have || g >= bg)) { bg = g; bc = c; have = 1; }
+                    } else {
+                        if (!have || g > bg) { bg = g; bc = c; have = 1; }
+                    }
+                }
+                if (bc >= 0 && bc != own && bg > 0.0f) prop[v] = bc;
+            }
+            free(acc); free(stamp); free(touched);
+        }
+        /* resolution from the pre-pass state, then the kept moves */
+        for (int64_t v = 0; v < n; v++) {
+            keep[v] = 0;
+            if (prop[v] == ref[v]) continue;
+            const int32_t t = prop[v];
+            const int t_proposes = ref[t] == t && rsz[t] == 1 && prop[t] != t;
+            keep[v] = !t_proposes || (prop[t] == (int32_t)v && t < (int32_t)v);
+        }
+        for (int64_t v = 0; v < n; v++) {
+            if (!keep[v]) continue;
+            const int32_t t = prop[v], o = ref[v];
+            aref[t] += s->k[v];
+            aref[o] -= s->k[v];
+            ref[v] = t;
+            rsz[t]++;
+            rsz[o]--;
+        }
+        const double qn = partition_modularity(s, ref, aref);
+        const double dq = qn - q;
+        q = qn;
+        p++;
+        s->refine_passes_run++;
+        if (!(dq > s->cfg.threshold) || p > s->cfg.max_iterations ||
+            (s->cfg.refine_passes > 0 && p >= s->cfg.refine_passes))
+            break;
+    }
+    free(prop); free(rsz); free(aref); free(wc); free(keep);
+    return ref;
+}
+
 /* OptimizationPhase::run (phaseOptimization.cuh:158-206) */
 int32_t orc_optimization_run(orc_state* s) {
     double delta;
@@ -472,17 +644,27 @@ int32_t orc_optimization_step(orc_state* s, double* delta) {
     return (int32_t)moved;
 }
 
-/* AggregationPhase::run (phaseAggregation.cuh:19-190) */
-int32_t orc_aggregation_run(orc_state* s, int32_t aggregate) {
+/* AggregationPhase::run (phaseAggregation.cuh:19-190). A refined run passes its refined
+ * partition in `ref` (taken over and freed): the level is aggregated by it. */
+static int32_t aggregate_by(orc_state* s, int32_t aggregate, int32_t* ref) {
     int64_t n = s->n;
+    if (!aggregate) { free(ref); ref = NULL; }
+    const int32_t* part = ref ? ref : s->comm;
     int32_t* map = (int32_t*)malloc((size_t)n * sizeof(int32_t));
-    if (!map) return ORC_ERR_NOMEM;
+    if (!map) { free(ref); return ORC_ERR_NOMEM; }
     int32_t run = 0;
-    for (int64_t c = 0; c < n; c++) { run += (s->a[c] > 0) ? 1 : 0; map[c] = run; }
+    if (s->cfg.refine) {
+        /* nonempty communities: labels with a member */
+        for (int64_t c = 0; c < n; c++) map[c] = 0;
+        for (int64_t v = 0; v < n; v++) map[part[v]] = 1;
+        for (int64_t c = 0; c < n; c++) { run += map[c]; map[c] = run; }
+    } else {
+        for (int64_t c = 0; c < n; c++) { run += (s->a[c] > 0) ? 1 : 0; map[c] = run; }
+    }
     /* community.h:48-55 update_best */
     for (int64_t v = 0; v < s->n0; v++) {
         int32_t b = s->best[v];
-        if (b >= 0 && b < n) s->best[v] = map[s->comm[b]] - 1;
+        if (b >= 0 && b < n) s->best[v] = map[part[b]] - 1;
     }
     s->n_best = run;
     if (!aggregate) { free(map); return ORC_OK; }
@@ -492,8 +674,8 @@ int32_t orc_aggregation_run(orc_state* s, int32_t aggregate) {
     int64_t* mptr = (int64_t*)calloc((size_t)n2 + 1, sizeof(int64_t));
     int32_t* members = (int32_t*)malloc((size_t)n * sizeof(int32_t));
     int32_t* newc = (int32_t*)malloc((size_t)n * sizeof(int32_t));
-    if (!mptr || !members || !newc) { free(map); free(mptr); free(members); free(newc); return ORC_ERR_NOMEM; }
-    for (int64_t v = 0; v < n; v++) { newc[v] = map[s->comm[v]] - 1; mptr[newc[v] + 1]++; }
+    if (!mptr || !members || !newc) { free(map); free(mptr); free(members); free(newc); free(ref); return ORC_ERR_NOMEM; }
+    for (int64_t v = 0; v < n; v++) { newc[v] = map[part[v]] - 1; mptr[newc[v] + 1]++; }
     for (int64_t c = 0; c < n2; c++) mptr[c + 1] += mptr[c];
     {
         int64_t* cur = (int64_t*)malloc((size_t)n2 * sizeof(int64_t));
@@ -549,27 +731,77 @@ int32_t orc_aggregation_run(orc_state* s, int32_t aggregate) {
             free(acc); free(stamp); free(touched);
         }
     }
-    free(map); free(mptr); free(members); free(newc); free(cnt);
+    /* refined: each new vertex remembers its members' coarse community */
+    int32_t* prev = NULL;
+    if (ref && !failed) {
+        int32_t* lab = (int32_t*)malloc((size_t)n * sizeof(int32_t));
+        prev = (int32_t*)malloc((size_t)(n2 > 0 ? n2 : 1) * sizeof(int32_t));
+        if (!lab || !prev) {
+            failed = 1;
+            free(prev);
+            prev = NULL;
+        } else {
+            for (int64_t c = 0; c < n; c++) lab[c] = INT32_MAX;
+            for (int64_t v = 0; v < n; v++)
+                if (newc[v] < lab[s->comm[v]]) lab[s->comm[v]] = newc[v];
+            for (int64_t v = 0; v < n; v++) prev[newc[v]] = lab[s->comm[v]];
+        }
+        free(lab);
+    }
+    free(map); free(mptr); free(members); free(newc); free(cnt); free(ref);
+    if (failed) free(prev);
     if (failed) { free(row2); free(col2); free(wi2); free(wf2); free(k2); return ORC_ERR_NOMEM; }
     free_graph(s);
     s->row_ptr = row2; s->col = col2; s->wi = wi2; s->wf = wf2; s->k = k2;
     s->n = n2; s->E = row2[n2];
     s->level++;
     level_reset(s);
+    if (prev) {
+        free(s->prev);
+        s->prev = prev;
+    }
     return ORC_OK;
 }
 
-/* ModularityAlgorithms::modularity_routine (modularityAlgorithms.h:14-81) */
+int32_t orc_aggregation_run(orc_state* s, int32_t aggregate) {
+    int32_t* ref = NULL;
+    if (aggregate && s->cfg.refine) {
+        ref = refine_partition(s);
+        if (!ref) return ORC_ERR_NOMEM;
+    }
+    return aggregate_by(s, aggregate, ref);
+}
+
+/* ModularityAlgorithms::modularity_routine (modularityAlgorithms.h:14-81); the refined
+ * continuation rule is in the header comment. */
 int32_t orc_louvain(orc_state* s) {
     int32_t levels = 0;
     int cont;
+    double prev_end = 0.0;
     do {
         double old = s->modularity;
+        if (s->cfg.refine && levels > 0) old = prev_end;
         orc_optimization_run(s);
         cont = (s->modularity - old) > s->cfg.threshold;
+        prev_end = s->modularity;
         levels++;
-        if (s->cfg.max_levels > 0 && levels >= s->cfg.max_levels) cont = 0;
-        int32_t rc = orc_aggregation_run(s, cont);
+        const int last = s->cfg.max_levels > 0 && levels >= s->cfg.max_levels;
+        int32_t* ref = NULL;
+        if (s->cfg.refine && !last) {
+            ref = refine_partition(s);
+            if (!ref) return -ORC_ERR_NOMEM;
+            int64_t labels = 0;  /* refined communities: labels still held by their vertex */
+            for (int64_t v = 0; v < s->n; v++) labels += ref[v] == (int32_t)v ? 1 : 0;
+            cont = labels < s->n &&
+                   (cont || (double)labels < s->cfg.refine_tolerance * (double)s->n);
+        }
+        if (last) cont = 0;
+        if (s->cfg.refine && !cont && s->level > 0 && s->prev && s->modularity < old) {
+            /* the last level ended below the previous one: keep the previous partition */
+            memcpy(s->comm, s->prev, (size_t)s->n * sizeof(int32_t));
+            s->modularity = old;
+        }
+        int32_t rc = aggregate_by(s, cont, ref);
         if (rc != ORC_OK) return -rc;
     } while (cont);
     return levels;
@@ -599,3 +831,4 @@ void orc_get_trace(const orc_state* s, orc_iter_record* out) {
     memcpy(out, s->trace, (size_t)s->trace_len * sizeof(orc_iter_record));
 }
 int32_t orc_record_size(void) { return (int32_t)sizeof(orc_iter_record); }
+int64_t orc_refine_passes(const orc_state* s) { return s->refine_passes_run; }

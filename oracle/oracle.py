@@ -30,6 +30,9 @@ class OrcConfig(ctypes.Structure):
         ("chunk_edges", ctypes.c_int64),
         ("nthreads", ctypes.c_int32),
         ("integer_weights", ctypes.c_int32),
+        ("refine", ctypes.c_int32),
+        ("refine_passes", ctypes.c_int32),
+        ("refine_tolerance", ctypes.c_double),
     ]
 
 
@@ -65,7 +68,8 @@ def lib():
         L.orc_aggregation_run.argtypes = [vp, ctypes.c_int32]
         L.orc_optimization_step.restype = ctypes.c_int32
         L.orc_optimization_step.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
-        for name in ("orc_n", "orc_E", "orc_n_best", "orc_trace_len", "orc_overrun_events"):
+        for name in ("orc_n", "orc_E", "orc_n_best", "orc_trace_len", "orc_overrun_events",
+                     "orc_refine_passes"):
             getattr(L, name).restype = ctypes.c_int64
             getattr(L, name).argtypes = [vp]
         L.orc_level.restype = ctypes.c_int32
@@ -94,7 +98,9 @@ class Oracle:
     def __init__(self, graph, mode: int = SORT, threshold: float = 1e-3,
                  fast_first: bool = True, chunk_edges: int = 50_000_000,
                  max_iterations: int = 1_000_000_000, max_levels: int = 0,
-                 nthreads: int = 1, integer_weights: Optional[bool] = None):
+                 nthreads: int = 1, integer_weights: Optional[bool] = None,
+                 refine: bool = False, refine_passes: int = 0,
+                 refine_tolerance: float = 0.95):
         L = lib()
         self._row = np.ascontiguousarray(graph.row_ptr, dtype=np.int64)
         self._col = np.ascontiguousarray(graph.col, dtype=np.int32)
@@ -103,7 +109,8 @@ class Oracle:
             integer_weights = w is None or bool(np.all(np.floor(w) == w))
         self._w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
         cfg = OrcConfig(mode, int(fast_first), max_iterations, max_levels, threshold,
-                        chunk_edges, nthreads, int(integer_weights))
+                        chunk_edges, nthreads, int(integer_weights), int(refine), refine_passes,
+                        refine_tolerance)
         err = ctypes.c_int32(0)
         self._h = L.orc_create(graph.n, _ptr(self._row), _ptr(self._col),
                                None if self._w is None else _ptr(self._w),
@@ -171,6 +178,11 @@ class Oracle:
     def overrun_events(self) -> int:
         """Times the reference's modularity scratch (community.h:69,85) would be too short."""
         return lib().orc_overrun_events(self._h)
+
+    @property
+    def refine_passes(self) -> int:
+        """Refinement passes run so far (refine=True)."""
+        return lib().orc_refine_passes(self._h)
 
     @property
     def n_best(self) -> int:

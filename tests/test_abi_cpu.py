@@ -78,6 +78,18 @@ def test_config_defaults_follow_reference_constants(lv):
     raw = lv.Config()
     lv.load_library().lv_config_default(raw)
     assert raw.use_graphs == 1 and raw.validate == 1 and raw.weight_mode == lv.WEIGHTS_AUTO
+    assert raw.refine == 0 and raw.refine_passes == 0 and raw.refine_tolerance == 0.95
+
+
+def test_refine_configuration_validated_before_device_work(lv):
+    L = lv.load_library()
+    for field, value in (("refine", 2), ("refine_passes", -1), ("refine_tolerance", 1.5),
+                         ("refine_tolerance", float("nan"))):
+        c = lv.config(refine=True)
+        setattr(c, field, value)
+        h = ctypes.c_void_p()
+        assert L.lv_create(0, ctypes.byref(c), ctypes.byref(h)) == 1  # LV_ERR_ARGUMENT
+        assert not h.value
 
 
 def test_status_strings(lv):
