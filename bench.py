@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--pool", type=int, default=64, help="served: distinct request graphs")
     ap.add_argument("--slots", type=int, default=16, help="served: concurrent server slots")
     ap.add_argument("--rates", default="10,50,200,1000,2000", help="served: arrival rates, req/s")
+    ap.add_argument("--refine", action="store_true",
+                    help="rmat / reference arm: Leiden-style refinement before each aggregation "
+                         "(lv_config.refine; host-driven level loop)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in degree-bin table (default: tune on a sample first)")
     ap.add_argument("--captured", type=int, default=-1, choices=[-1, 0, 1],
@@ -190,7 +193,7 @@ def cpu_sample(args):
     import oracle as O
     g = build_graph(args.cpu_sample_scale)
     t = time.perf_counter()
-    o = O.Oracle(g, mode=O.SORT if args.mode == "SORT" else O.HASH, nthreads=1)
+    o = O.Oracle(g, mode=O.SORT if args.mode == "SORT" else O.HASH, nthreads=1, refine=args.refine)
     o.louvain()
     dt = time.perf_counter() - t
     return {"value": g.m / dt, "unit": "edges/s", "cores": 1, "kind": "port",
@@ -207,11 +210,11 @@ def run_reference(args, world, rank):
     threads = os.cpu_count() or 1
     mode = O.SORT if args.mode == "SORT" else O.HASH
     for _ in range(args.warmup):
-        O.Oracle(g, mode=mode, nthreads=threads).louvain()
+        O.Oracle(g, mode=mode, nthreads=threads, refine=args.refine).louvain()
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        o = O.Oracle(g, mode=mode, nthreads=threads)
+        o = O.Oracle(g, mode=mode, nthreads=threads, refine=args.refine)
         o.louvain()
         times.append(time.perf_counter() - t)
     sec = sum(times) / len(times)
@@ -222,7 +225,7 @@ def run_reference(args, world, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32+f64",
         "data": "synthetic",
         "config": {"workload": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "mode": args.mode,
-                   "threshold": 1e-3},
+                   "threshold": 1e-3, "refine": bool(args.refine)},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "port",
                          "sample": f"the full workload graph per step, oracle/louvain_oracle.c "
                                    f"with {threads} OpenMP threads (the reference has no CPU path)"},
@@ -503,6 +506,8 @@ def main():
     g = build_graph(args.scale, device=dev)
     mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
     kw = {} if args.captured < 0 else {"use_graphs": bool(args.captured)}
+    if args.refine:
+        kw["refine"] = True
     eng = lv.Engine(local, mode=mode, **kw)
     tune = {}
     if not args.no_autotune and not args.once:
@@ -576,10 +581,11 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 weights, f32 gains, f64 totals", "data": "synthetic",
         "config": {"workload": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "mode": args.mode,
-                   "threshold": 1e-3, "parallelism": "replicas" if world > 1 else "single",
+                   "threshold": 1e-3, "refine": bool(args.refine),
+                   "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (CSR 1.03 GB)"},
         "modularity": q, "n_communities": st.n_communities, "levels": st.levels,
-        "passes": st.iterations,
+        "passes": st.iterations, "refine_passes": st.refine_passes,
         "window_ms": st.ms_window, "optimization_ms": st.ms_optimization,
         "aggregation_ms": st.ms_aggregation, "wall_ms_per_step": wall / args.steps * 1e3,
         "e2e": {"value": world * g.m / e2e_sec, "unit": "edges/s",

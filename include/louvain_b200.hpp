@@ -122,6 +122,14 @@ class Engine {
     if (s != LV_OK) throw Error(s, std::string("lv_create: ") + lv_status_string(s));
     ctx_.reset(ctx);
   }
+  // Any configuration (e.g. refine = 1 for the Leiden-style refinement); start from
+  // lv_config_default.
+  explicit Engine(const lv_config& cfg, int device = 0) {
+    lv_context* ctx = nullptr;
+    const lv_status s = lv_create(device, &cfg, &ctx);
+    if (s != LV_OK) throw Error(s, std::string("lv_create: ") + lv_status_string(s));
+    ctx_.reset(ctx);
+  }
   Community run(const GraphHost& g) {
     Community C;
     std::vector<int32_t> out(g.n_nodes);
