@@ -90,6 +90,7 @@ struct Ctrl {
   uint32_t long_count;         // aggregation: pieces of long rows for k_hub_insert_long
   uint32_t long_movers;        // pass: team-kernel movers with long rows, for k_apply_long
   uint32_t hub_members;        // aggregation: members of the bin-7 communities, for k_hub_insert
+  uint32_t hub_work;           // aggregation: next group of bin-7 members a k_hub_insert warp takes
   uint32_t hub_items;          // pass: pieces of the bin-7 (global-table) vertices' rows
   uint32_t apply_items;        // pass: pieces of the rows of movers found by block kernels
   uint32_t hub_cursor;         // global hash-table arena cursor (slots)

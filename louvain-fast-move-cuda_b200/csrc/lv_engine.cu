@@ -514,7 +514,7 @@ class Run {
     D.hub_off = dalloc<uint32_t>(ctx, owned, n);
     D.hubtab = dalloc<uint32_t>(ctx, owned, n);
     D.hubself = dalloc<unsigned long long>(ctx, owned, n);
-    D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
+    D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / std::min(kHubPiece, kHubInsPiece) + 16);
     D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
     D.movers = dalloc<uint32_t>(ctx, owned, n);
     D.gs = dalloc<GraphState>(ctx, owned, G);

@@ -81,8 +81,12 @@ struct BinCfg {
 
 // Table granule of the multi-block global tables: every global table is a multiple of it.
 constexpr uint32_t kHubChunk = 4096;
-// Rows longer than kHubLongRow entries are inserted in pieces of kHubPiece by separate blocks.
-constexpr uint32_t kHubLongRow = 2048;
+// In the contraction's global tables, rows longer than kHubLongRow entries are inserted in
+// pieces of kHubInsPiece by separate blocks (k_hub_insert_long); shorter ones by warps taking
+// 32 member rows at a time (k_hub_insert). At R-MAT scale 22 a 256-entry split costs 5.2 ms
+// for both kernels against 6.0 ms with 2048 (one warp per 2048-entry piece: 6.1 ms).
+constexpr uint32_t kHubLongRow = 256;
+constexpr uint32_t kHubInsPiece = 8192;
 constexpr uint32_t kHubPiece = 8192;
 
 constexpr int kMaxPartials = 2048;
@@ -1614,8 +1618,6 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
   const uint32_t* hubs = D.bins[kNumBins - 1];
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   const int lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t err = 0;
   // entries staying inside their community are summed in registers
   uint32_t self_s = kEmpty;  // per-lane running self-loop sum, flushed when the community changes
@@ -1638,7 +1640,12 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
     }
     if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
   };
-  for (uint32_t pb = warp * 32u; pb < total; pb += nwarps * 32u) {
+  // warps take groups of 32 members from a shared counter (row lengths are heavy-tailed)
+  for (;;) {
+    uint32_t pb = 0;
+    if (lane == 0) pb = atomicAdd(&C->hub_work, 32u);
+    pb = __shfl_sync(kFull, pb, 0);
+    if (pb >= total) break;
     const uint32_t p = pb + lane;
     uint32_t rs = 0, len = 0, s = 0, off = 0, cap = 0;
     if (p < total) {
@@ -1660,7 +1667,7 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
         len = D.row[v + 1] - rs;
         if (len > kHubLongRow) {
           // long rows are cut into pieces that separate blocks insert (k_hub_insert_long)
-          const uint32_t np = (len + kHubPiece - 1) / kHubPiece;
+          const uint32_t np = (len + kHubInsPiece - 1) / kHubInsPiece;
           const uint32_t p0 = atomicAdd(&C->long_count, np);
           for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
           len = 0;
@@ -1699,8 +1706,8 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
     const uint32_t dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
     const uint32_t cap = contract_cap(dsum, D.gs[g].n_next, true);
     if (off == kEmpty || (unsigned long long)off + cap > C->arena_slots) { err |= kErrIndex; continue; }
-    const uint32_t rs = D.row[v] + piece * kHubPiece;
-    const uint32_t re = min(D.row[v + 1], rs + kHubPiece);
+    const uint32_t rs = D.row[v] + piece * kHubInsPiece;
+    const uint32_t re = min(D.row[v + 1], rs + kHubInsPiece);
     Acc self_acc = Acc(0);
     for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
       const uint32_t d = D.new_comm[D.col[e]];
@@ -2169,6 +2176,7 @@ __global__ void k_agg_clear_next(int dslot) {
     for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
     C->long_count = 0;  // k_hub_insert queues this aggregation's long rows from zero
+    C->hub_work = 0;    // and takes its member groups from zero
   }
 }
 // The global contraction tables of this aggregation: empty keys, zero values.

@@ -184,3 +184,66 @@ def test_refine_configuration_errors(lv, graphs):
     c.close()
     e.close()
     e2.close()
+
+
+# ---- structured edge cases -------------------------------------------------------------------------
+def _with_self_loops(g, every=7, weight=3.0):
+    """Adds a self-loop entry of `weight` to every `every`-th vertex (kept sorted by column)."""
+    import numpy as np
+    from importlib import import_module
+    CSRGraph = import_module("louvain-fast-move-cuda_b200.graphs").CSRGraph
+    src = g.src()
+    w = g.weights_or_ones.astype(np.float32)
+    loops = np.arange(0, g.n, every)
+    s2 = np.concatenate([src, loops])
+    c2 = np.concatenate([g.col.astype(np.int64), loops])
+    w2 = np.concatenate([w, np.full(loops.size, weight, dtype=np.float32)])
+    order = np.lexsort((c2, s2))
+    s2, c2, w2 = s2[order], c2[order], w2[order]
+    row = np.zeros(g.n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(s2, minlength=g.n), out=row[1:])
+    return CSRGraph(n=g.n, row_ptr=row, col=c2.astype(np.int32), w=w2, name=g.name + "_loops")
+
+
+def _edge_case(name, graphs):
+    rng = np.random.default_rng(3)
+    if name == "stars":
+        u = np.concatenate([np.zeros(200), np.full(150, 201), [0]])
+        v = np.concatenate([np.arange(1, 201), np.arange(202, 352), [201]])
+        return graphs.canonical_from_pairs(u, v, name="stars")
+    if name == "ring_of_cliques":
+        us, vs = [], []
+        for c in range(30):
+            b = 6 * c
+            for i in range(6):
+                for j in range(i + 1, 6):
+                    us.append(b + i)
+                    vs.append(b + j)
+            us.append(b)
+            vs.append((b + 6) % 180)
+        return graphs.canonical_from_pairs(np.array(us), np.array(vs), name="ring_of_cliques")
+    if name == "int_weights":
+        g = graphs.chung_lu_bounded(5000, 2.0, 1, 99, seed=12)
+        src = g.src()
+        key = np.minimum(src, g.col) * 7919 + np.maximum(src, g.col)
+        g.w = (key % 5 + 1).astype(np.float32)  # symmetric integer weights 1..5
+        return g
+    if name == "self_loops":
+        return _with_self_loops(graphs.chung_lu_bounded(4000, 2.0, 1, 99, seed=13))
+    if name == "components":
+        a = graphs.rmat(10, 8, seed=4)
+        b = _edge_case("ring_of_cliques", graphs)
+        u = np.concatenate([a.src(), b.src() + a.n])
+        v = np.concatenate([a.col, b.col + a.n])
+        return graphs.canonical_from_pairs(u, v, name="components")
+    raise KeyError(name)
+
+
+EDGE_CASES = ["stars", "ring_of_cliques", "int_weights", "self_loops", "components"]
+
+
+@pytest.mark.parametrize("name", EDGE_CASES)
+def test_refine_edge_cases(name, lv, oracle, graphs):
+    g = _edge_case(name, graphs)
+    for mode in (1, 0):
+        _check_full(lv, oracle, g, mode)

@@ -69,3 +69,28 @@ def test_refine_off_is_the_plain_run(oracle, graphs):
     b.louvain()
     np.testing.assert_array_equal(a.best(), b.best())
     assert a.modularity == b.modularity and b.refine_passes == 0
+
+
+@pytest.mark.parametrize("name", ["stars", "ring_of_cliques", "int_weights", "self_loops", "components"])
+def test_refined_partition_edge_cases(name, oracle, graphs):
+    from test_refine_gpu import _edge_case
+    g = _edge_case(name, graphs)
+    o = oracle.Oracle(g, mode=1, refine=True)
+    o.optimization_run()
+    coarse = o.comm()
+    o.aggregation_run(True)
+    _components_ok(g, o.best(), coarse)
+    full = oracle.Oracle(g, mode=1, refine=True)
+    full.louvain()
+    assert np.unique(full.best()).size == full.n_best
+
+
+def test_ring_of_cliques_keeps_cliques(oracle, graphs):
+    """30 six-cliques in a ring: every final community is a union of whole cliques."""
+    from test_refine_gpu import _edge_case
+    g = _edge_case("ring_of_cliques", graphs)
+    o = oracle.Oracle(g, mode=1, refine=True)
+    o.louvain()
+    b = o.best()
+    for c in range(30):
+        assert np.unique(b[6 * c:6 * c + 6]).size == 1
