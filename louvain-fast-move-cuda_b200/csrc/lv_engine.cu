@@ -780,9 +780,12 @@ class Run {
     const uint32_t ml = (uint32_t)std::max(0, cfg.max_levels);
     k_ref_init<<<grid_n, 256, 0, st>>>(Dd, ml);
     k_ref_count<WI><<<grid_n, 256, 0, st>>>(Dd);
+    k_ref_count_long<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     scan<uint32_t, false, kScanDeg>();
+    k_ref_elig_long<WI><<<ctx->sms, 256, 0, st>>>(Dd);
     k_ref_fill<WI><<<grid_n, 256, 0, st>>>(Dd);
-    launches += 3;
+    k_ref_fill_long<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
+    launches += 6;
     // The restricted rows are no longer than the level's rows, so the level start's arena
     // already holds every global table a refinement pass can need.
     bind_refine();

@@ -36,6 +36,10 @@ namespace lv {
 
 constexpr uint32_t kRefEligible = 1u;  // rflag: well connected to its community at the start
 constexpr uint32_t kRefReject = 2u;    // rflag: this pass's proposal was not kept
+// Rows longer than kRefLong entries are restricted in pieces of kHubPiece entries, one block
+// per piece (queued in long_items, counted by long_count, both free until the aggregation):
+// a warp per row would leave the GPU waiting on a few hub rows.
+constexpr uint32_t kRefLong = 1024;
 
 // Set-up of a refinement (main view). Graphs that aggregate now and are below the level cap
 // refine (gsR[g].agg = 1, phase kIterating); the others sit it out (kFinished). The chunk
@@ -68,7 +72,22 @@ __global__ void k_ref_init(int dslot, uint32_t max_levels) {
   if (tid == 0) {
     C->chunk_on = 0;
     C->n_next = n;  // length of the row-offset scan (kScanDeg scans n_next + 1 entries)
+    C->long_count = 0;
   }
+}
+
+// The eligibility test 2m w(v, S - v) >= k_v (K_S - k_v), K_S = a[S]: exact in 128-bit integers
+// (2m, k_v, K_S and w(v, S - v) are integers below 2^33), in double for fp32 weights.
+template <bool WINT>
+__device__ __forceinline__ bool ref_well_connected(const Dev& D, uint32_t v, uint32_t g, uint32_t cv,
+                                                   unsigned long long wi, double wf) {
+  const double m = D.gsR[g].m, kv = D.k[v], K = D.a[cv];
+  if (WINT) {
+    const unsigned long long two_m = (unsigned long long)__dmul_rn(2.0, m);
+    const unsigned long long ki = (unsigned long long)kv, Ki = (unsigned long long)K;
+    return (unsigned __int128)two_m * wi >= (unsigned __int128)ki * (Ki - ki);
+  }
+  return __dmul_rn(__dmul_rn(2.0, m), wf) >= __dmul_rn(kv, __dsub_rn(K, kv));
 }
 
 // Per vertex of a refining graph, one warp per vertex (main view): its entries inside its
@@ -92,6 +111,17 @@ __global__ void __launch_bounds__(256) k_ref_count(int dslot) {
       continue;
     }
     const uint32_t cv = D.comm[v], rs = D.row[v], re = D.row[v + 1];
+    if (re - rs > kRefLong) {
+      // pieces for k_ref_count_long, which adds into newdeg[v] and hubself[v]
+      if (lane == 0) {
+        const uint32_t np = (re - rs + kHubPiece - 1) / kHubPiece;
+        const uint32_t p0 = atomicAdd(&C->long_count, np);
+        for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
+        D.newdeg[v] = 0;
+        D.hubself[v] = 0ull;
+      }
+      continue;
+    }
     uint32_t cnt = 0;
     unsigned long long wi = 0, si = 0;
     double wf = 0.0, sf = 0.0;
@@ -110,23 +140,83 @@ __global__ void __launch_bounds__(256) k_ref_count(int dslot) {
     else { wf = warp_sum(wf); sf = warp_sum(sf); }
     if (lane == 0) {
       D.newdeg[v] = cnt;
-      const GraphState& r = D.gsR[g];
-      const double kv = D.k[v], K = D.a[cv];
-      bool ok;
       if (WINT) {
-        // 2m, k_v, K_S and w(v, S - v) are integers below 2^33: compare exactly in 128 bits
-        const unsigned long long two_m = (unsigned long long)__dmul_rn(2.0, r.m);
-        const unsigned long long ki = (unsigned long long)kv, Ki = (unsigned long long)K;
-        ok = (unsigned __int128)two_m * wi >= (unsigned __int128)ki * (Ki - ki);
         if (si) atomicAdd(&D.gsR[g].I, si);
-      } else {
-        ok = __dmul_rn(__dmul_rn(2.0, r.m), wf) >= __dmul_rn(kv, __dsub_rn(K, kv));
-        if (sf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gsR[g].I), sf);
+      } else if (sf != 0.0) {
+        atomicAdd(reinterpret_cast<double*>(&D.gsR[g].I), sf);
       }
-      D.rflag[v] = ok ? kRefEligible : 0u;
+      D.rflag[v] = ref_well_connected<WINT>(D, v, g, cv, wi, wf) ? kRefEligible : 0u;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) D.newdeg[n] = 0;
+}
+
+// A piece of a long row (main view), one block each: its kept entries, intra-community weight
+// (into hubself[v]) and self-loop weight.
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_ref_count_long(int dslot) {
+  const Dev& D = c_dev[dslot];
+  using Tr = WTraits<WINT>;
+  using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  __shared__ unsigned long long shu[33];
+  __shared__ double shd[33];
+  __shared__ uint32_t shc[33];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->long_count, n = C->n;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const unsigned long long it = D.long_items[idx];
+    const uint32_t v = (uint32_t)(it >> 32), piece = (uint32_t)it;
+    if (v >= n) continue;  // never: k_ref_count queued it
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    const uint32_t cv = D.comm[v];
+    const uint32_t rs = D.row[v] + piece * kHubPiece, re = min(D.row[v + 1], rs + kHubPiece);
+    uint32_t cnt = 0;
+    unsigned long long wi = 0, si = 0;
+    double wf = 0.0, sf = 0.0;
+    for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
+      const uint32_t u = D.col[e];
+      if (D.comm[u] != cv) continue;
+      ++cnt;
+      if (WINT) {
+        if (u == v) si += (unsigned long long)w[e]; else wi += (unsigned long long)w[e];
+      } else {
+        if (u == v) sf += Tr::w_double(w[e]); else wf += Tr::w_double(w[e]);
+      }
+    }
+    cnt = block_sum<256>(cnt, shc);
+    if (WINT) { wi = block_sum<256>(wi, shu); si = block_sum<256>(si, shu); }
+    else { wf = block_sum<256>(wf, shd); sf = block_sum<256>(sf, shd); }
+    if (threadIdx.x == 0) {
+      if (cnt) atomicAdd(&D.newdeg[v], cnt);
+      if (WINT) {
+        if (wi) atomicAdd(&D.hubself[v], wi);
+        if (si) atomicAdd(&D.gsR[g].I, si);
+      } else {
+        if (wf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.hubself[v]), wf);
+        if (sf != 0.0) atomicAdd(reinterpret_cast<double*>(&D.gsR[g].I), sf);
+      }
+    }
+  }
+}
+
+// Eligibility of the long rows, once their pieces are summed (main view): one thread per row
+// (its first piece).
+template <bool WINT>
+__global__ void k_ref_elig_long(int dslot) {
+  const Dev& D = c_dev[dslot];
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->long_count, n = C->n;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+    const unsigned long long it = D.long_items[idx];
+    const uint32_t v = (uint32_t)(it >> 32), piece = (uint32_t)it;
+    if (piece != 0 || v >= n) continue;
+    const uint32_t g = D.gid ? D.gid[v] : 0u;
+    const unsigned long long acc = D.hubself[v];
+    D.rflag[v] = ref_well_connected<WINT>(D, v, g, D.comm[v], acc, __longlong_as_double((long long)acc))
+                     ? kRefEligible : 0u;
+    D.rank[v] = D.rowB[v];  // k_ref_fill_long's output cursor (rank is free until the aggregation)
+  }
 }
 
 // The restricted rows (main view): entries inside the vertex's community, in row order, to
@@ -146,6 +236,7 @@ __global__ void __launch_bounds__(256) k_ref_fill(int dslot) {
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     if (D.gsR[g].phase != kIterating) continue;
     const uint32_t cv = D.comm[v], rs = D.row[v], re = D.row[v + 1];
+    if (re - rs > kRefLong) continue;  // k_ref_fill_long
     uint32_t out = D.rowB[v];
     for (uint32_t b = rs; b < re; b += 32) {
       const uint32_t e = b + lane;
@@ -162,6 +253,51 @@ __global__ void __launch_bounds__(256) k_ref_fill(int dslot) {
         wo[p] = w[e];
       }
       out += __popc(m);
+    }
+  }
+}
+
+// The long rows' pieces (main view), one block each: kept entries are placed through the row's
+// cursor (rank[v]), one atomic per warp and 32 entries. Their order inside the row is not the
+// level's; nothing depends on it (the refinement passes are table passes, their sums exact
+// with integer weights).
+template <bool WINT>
+__global__ void __launch_bounds__(256) k_ref_fill_long(int dslot) {
+  const Dev& D = c_dev[dslot];
+  using Wt = typename WTraits<WINT>::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  Wt* __restrict__ wo = reinterpret_cast<Wt*>(D.wB);
+  Ctrl* C = D.ctrl;
+  const uint32_t count = C->long_count, n = C->n;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const unsigned long long it = D.long_items[idx];
+    const uint32_t v = (uint32_t)(it >> 32), piece = (uint32_t)it;
+    if (v >= n) continue;
+    const uint32_t cv = D.comm[v];
+    const uint32_t rs = D.row[v] + piece * kHubPiece, re = min(D.row[v + 1], rs + kHubPiece);
+    const uint32_t lim = D.rowB[v + 1];
+    // warp-uniform trip count: every lane takes part in each ballot
+    for (uint32_t b = rs + (threadIdx.x & ~31u); b < re; b += blockDim.x) {
+      const uint32_t e = b + lane;
+      uint32_t u = 0;
+      bool keep = false;
+      if (e < re) {
+        u = D.col[e];
+        keep = D.comm[u] == cv;
+      }
+      const unsigned m = __ballot_sync(kFull, keep);
+      if (!m) continue;
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&D.rank[v], (uint32_t)__popc(m));
+      base = __shfl_sync(kFull, base, 0);
+      if (keep) {
+        const uint32_t p = base + __popc(m & lanemask_lt());
+        if (p < lim) {
+          D.colB[p] = u;
+          wo[p] = w[e];
+        }
+      }
     }
   }
 }
