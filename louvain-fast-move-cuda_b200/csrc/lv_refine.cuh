@@ -90,62 +90,72 @@ __device__ __forceinline__ bool ref_well_connected(const Dev& D, uint32_t v, uin
   return __dmul_rn(__dmul_rn(2.0, m), wf) >= __dmul_rn(kv, __dsub_rn(K, kv));
 }
 
-// Per vertex of a refining graph, one warp per vertex (main view): its entries inside its
-// community (the restricted row length, in newdeg for the offsets scan), the eligibility test
-// and its self-loop weight (the singleton partition's internal weight).
+// Per vertex of a refining graph, a team of kRefT lanes per vertex (main view): its entries
+// inside its community (the restricted row length, in newdeg for the offsets scan), the
+// eligibility test and its self-loop weight (the singleton partition's internal weight).
+// Rows longer than kRefLong are queued in pieces for k_ref_count_long.
+constexpr int kRefT = 8;
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_ref_count(int dslot) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Wt = typename Tr::W;
+  using Acc = typename Tr::Acc;  // a row's weight sum is at most k_v
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, tl = lane & (kRefT - 1);
+  constexpr uint32_t kPerWarp = 32 / kRefT;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = warp; v < n; v += nwarps) {
-    const uint32_t g = D.gid ? D.gid[v] : 0u;
-    if (D.gsR[g].phase != kIterating) {
-      if (lane == 0) D.newdeg[v] = 0;
-      continue;
-    }
-    const uint32_t cv = D.comm[v], rs = D.row[v], re = D.row[v + 1];
-    if (re - rs > kRefLong) {
-      // pieces for k_ref_count_long, which adds into newdeg[v] and hubself[v]
-      if (lane == 0) {
-        const uint32_t np = (re - rs + kHubPiece - 1) / kHubPiece;
-        const uint32_t p0 = atomicAdd(&C->long_count, np);
-        for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
-        D.newdeg[v] = 0;
-        D.hubself[v] = 0ull;
+  // warp-uniform trip count: every lane reaches the team sums
+  for (uint32_t vb = warp * kPerWarp; vb < n; vb += nwarps * kPerWarp) {
+    const uint32_t v = vb + (uint32_t)(lane / kRefT);
+    bool live = v < n;
+    uint32_t g = 0, cv = 0, rs = 0, re = 0;
+    if (live) {
+      g = D.gid ? D.gid[v] : 0u;
+      if (D.gsR[g].phase != kIterating) {
+        if (tl == 0) D.newdeg[v] = 0;
+        live = false;
+      } else {
+        cv = D.comm[v];
+        rs = D.row[v];
+        re = D.row[v + 1];
+        if (re - rs > kRefLong) {
+          // pieces for k_ref_count_long, which adds into newdeg[v] and hubself[v]
+          if (tl == 0) {
+            const uint32_t np = (re - rs + kHubPiece - 1) / kHubPiece;
+            const uint32_t p0 = atomicAdd(&C->long_count, np);
+            for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)v << 32) | k;
+            D.newdeg[v] = 0;
+            D.hubself[v] = 0ull;
+          }
+          live = false;
+        }
       }
-      continue;
     }
     uint32_t cnt = 0;
-    unsigned long long wi = 0, si = 0;
-    double wf = 0.0, sf = 0.0;
-    for (uint32_t e = rs + lane; e < re; e += 32) {
-      const uint32_t u = D.col[e];
-      if (D.comm[u] != cv) continue;
-      ++cnt;
-      if (WINT) {
-        if (u == v) si += (unsigned long long)w[e]; else wi += (unsigned long long)w[e];
-      } else {
-        if (u == v) sf += Tr::w_double(w[e]); else wf += Tr::w_double(w[e]);
+    Acc wi = Acc(0), si = Acc(0);
+    if (live) {
+      for (uint32_t e = rs + tl; e < re; e += kRefT) {
+        const uint32_t u = D.col[e];
+        if (D.comm[u] != cv) continue;
+        ++cnt;
+        if (u == v) si += (Acc)w[e]; else wi += (Acc)w[e];
       }
     }
-    cnt = warp_sum(cnt);
-    if (WINT) { wi = warp_sum(wi); si = warp_sum(si); }
-    else { wf = warp_sum(wf); sf = warp_sum(sf); }
-    if (lane == 0) {
+    cnt = team_sum<kRefT>(cnt);
+    wi = team_sum<kRefT>(wi);
+    si = team_sum<kRefT>(si);
+    if (live && tl == 0) {
       D.newdeg[v] = cnt;
-      if (WINT) {
-        if (si) atomicAdd(&D.gsR[g].I, si);
-      } else if (sf != 0.0) {
-        atomicAdd(reinterpret_cast<double*>(&D.gsR[g].I), sf);
+      if (si != Acc(0)) {
+        if (WINT) atomicAdd(&D.gsR[g].I, (unsigned long long)si);
+        else atomicAdd(reinterpret_cast<double*>(&D.gsR[g].I), (double)si);
       }
-      D.rflag[v] = ref_well_connected<WINT>(D, v, g, cv, wi, wf) ? kRefEligible : 0u;
+      D.rflag[v] = ref_well_connected<WINT>(D, v, g, cv, (unsigned long long)wi, (double)wi)
+                       ? kRefEligible : 0u;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) D.newdeg[n] = 0;
@@ -220,8 +230,9 @@ __global__ void k_ref_elig_long(int dslot) {
 }
 
 // The restricted rows (main view): entries inside the vertex's community, in row order, to
-// rowB/colB/wB (offsets from the scan of k_ref_count's counts). One warp per vertex; a ballot
-// per 32 entries places the kept ones.
+// rowB/colB/wB (offsets from the scan of k_ref_count's counts). One warp per row, a ballot per
+// 32 entries places the kept ones (teams of kRefT lanes, as in k_ref_count, were slower here:
+// 3.7 against 2.3 ms at R-MAT scale 22). Long rows are left to k_ref_fill_long.
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_ref_fill(int dslot) {
   const Dev& D = c_dev[dslot];
