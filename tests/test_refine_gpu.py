@@ -247,3 +247,18 @@ def test_refine_edge_cases(name, lv, oracle, graphs):
     g = _edge_case(name, graphs)
     for mode in (1, 0):
         _check_full(lv, oracle, g, mode)
+
+
+@pytest.mark.slow
+def test_refine_rmat22_matches_oracle(lv, oracle, golden):
+    """Full-size workload (R-MAT scale 22, 128.3 M entries, chunking active in the levels'
+    passes): the refined run's partition, community count and modularity equal the oracle's."""
+    g = golden.case_graph(golden.RMAT22)
+    e = lv.Engine(0, mode=1, refine=True)
+    best, q, st = e.run_graph(g)
+    o = _oracle_run(oracle, g)
+    np.testing.assert_array_equal(best, o.best())
+    assert st.n_communities == o.n_best
+    assert abs(q - o.modularity) <= Q_TOL
+    assert st.refine_passes == o.refine_passes
+    e.close()
