@@ -1605,8 +1605,9 @@ __global__ void __launch_bounds__(1024) k_hub_member_prefix(int dslot) {
 }
 
 // Bin-7 insert: the members of all large communities at once (and no other vertex), 32 per
-// warp, their rows spread over the lanes, into their communities' global tables (L2 atomics).
-// Long rows go to k_hub_insert_long in pieces.
+// warp (groups taken from a shared counter), their rows spread over the lanes, into their
+// communities' global tables (L2 atomics). Rows over kHubLongRow go to k_hub_insert_long in
+// pieces.
 template <bool WINT>
 __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
   const Dev& D = c_dev[dslot];
