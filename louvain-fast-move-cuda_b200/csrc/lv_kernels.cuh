@@ -270,10 +270,7 @@ __device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
 constexpr int kBatch = 4;
 // The apply kernels' gathers per lane in flight: their chains are short and register-light,
 // so they take twice the optimisation kernels' depth (8 vs 4: 6 % less apply time at scale 22).
-#ifndef LV_APPLY_BATCH
-#define LV_APPLY_BATCH 8
-#endif
-constexpr int kApplyBatch = LV_APPLY_BATCH;
+constexpr int kApplyBatch = 8;
 
 // Fast pass: best key over positive per-entry gains (self = 0, destination's own total).
 template <bool WINT>
