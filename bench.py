@@ -413,7 +413,8 @@ def run_served(args, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 weights, f32 gains, f64 totals", "data": "synthetic",
         "config": {"workload": "rmat_ef8_n1000-2000000_poisson", "pool": len(pool),
-                   "mean_m": float(np.mean([g.m for g in pool])), "slots": args.slots,
+                   "mean_m": float(np.mean([g.m for g in pool])),
+                   "pool_entries": int(sum(g.E for g in pool)), "slots": args.slots,
                    "budget_gb": 150, "mode": "SORT"},
         "rates": rates, "p50_ms_at_best": best["p50_ms"], "p99_ms_at_best": best["p99_ms"],
         "loop": {"graphs_per_s": loop_gps, "what": "the pool once, one lv_run_csr call per "
