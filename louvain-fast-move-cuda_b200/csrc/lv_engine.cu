@@ -517,6 +517,7 @@ class Run {
     D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / std::min(kHubPiece, kHubInsPiece) + 16);
     D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
     D.movers = dalloc<uint32_t>(ctx, owned, n);
+    D.cn = dalloc<unsigned long long>(ctx, owned, n);
     D.gs = dalloc<GraphState>(ctx, owned, G);
     D.ctrl = dalloc<Ctrl>(ctx, owned, 1);
     D.partials = dalloc<double>(ctx, owned, kMaxPartials);
@@ -700,12 +701,13 @@ class Run {
       launches += 2;
     }
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[5], st));
+    k_pack_cn<<<grid_n, 256, 0, st>>>(Dd);
     k_apply<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_long<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
     commit_sq();
     finalize(0, view);
-    launches += 18;
+    launches += 19;
   }
 
   // Runs one pass; returns the number of graphs still iterating.

@@ -56,6 +56,7 @@ struct Dev {
   uint32_t* gid0;            // [n0] graph of each input vertex (nullptr: one graph)
   int32_t* out;              // [n0] final community ids
   unsigned long long* scan_tmp;  // [(n + 1) / kScanTile + 2] tile sums of the scans
+  unsigned long long* cn;    // [n] apply phase: (new_comm << 32) | comm, one gather per entry
   // refinement (allocated only when it is on; lv_refine.cuh)
   uint32_t* ref;             // [n] refined partition
   uint32_t* ref_new;         // [n] its pass targets
@@ -719,8 +720,9 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
     }
 #pragma unroll
     for (int k = 0; k < kApplyBatch; ++k) {
-      pre[k] = uu[k] != kEmpty ? D.comm[uu[k]] : 0u;
-      nc[k] = uu[k] != kEmpty ? D.new_comm[uu[k]] : 0u;
+      const unsigned long long x = uu[k] != kEmpty ? D.cn[uu[k]] : 0ull;
+      pre[k] = (uint32_t)x;
+      nc[k] = (uint32_t)(x >> 32);
     }
 #pragma unroll
     for (int k = 0; k < kApplyBatch; ++k) {
@@ -748,6 +750,15 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
 // to k_apply_long (a warp each; movers sit in the list grouped by degree, so a warp taking 32
 // long rows would hold up the whole kernel). An entry's change of the internal weight goes to
 // its own graph, which is the mover's (edges never cross graphs).
+// Before the apply kernels: each vertex's pre-pass community and this pass's target packed
+// in one word, so that an entry costs one 8-byte gather instead of two 4-byte ones.
+__global__ void k_pack_cn(int dslot) {
+  const Dev& D = c_dev[dslot];
+  const uint32_t n = D.ctrl->n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    D.cn[v] = ((unsigned long long)D.new_comm[v] << 32) | D.comm[v];
+}
+
 constexpr uint32_t kApplyShort = 32;
 
 template <bool WINT>
@@ -827,8 +838,9 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
       }
 #pragma unroll
       for (int q = 0; q < kApplyBatch; ++q) {
-        pre[q] = uu[q] != kEmpty ? D.comm[uu[q]] : 0u;
-        nc[q] = uu[q] != kEmpty ? D.new_comm[uu[q]] : 0u;
+        const unsigned long long x = uu[q] != kEmpty ? D.cn[uu[q]] : 0ull;
+        pre[q] = (uint32_t)x;
+        nc[q] = (uint32_t)(x >> 32);
       }
 #pragma unroll
       for (int q = 0; q < kApplyBatch; ++q) {
