@@ -46,3 +46,59 @@ def test_oracle_refine_second_level_and_pass_limit(oracle, graphs):
                           a.tolist(), o.total_weight, mode=1, max_passes=cap)
         o.aggregation_run(True)
         np.testing.assert_array_equal(o.best(), R.renumber(labels)[best0])
+
+
+def _random_graph(seed: int, n: int, p: float, loops: bool):
+    """A random symmetric CSR with integer weights 1..3 and optional self-loop entries."""
+    from importlib import import_module
+    CSRGraph = import_module("louvain-fast-move-cuda_b200.graphs").CSRGraph
+    rng = np.random.default_rng(seed)
+    src, dst, wts = [], [], []
+    for u in range(n):
+        for v in range(u + 1, n):
+            if rng.random() < p:
+                w = float(rng.integers(1, 4))
+                src += [u, v]
+                dst += [v, u]
+                wts += [w, w]
+        if loops and rng.random() < 0.2:
+            src.append(u)
+            dst.append(u)
+            wts.append(float(rng.integers(1, 4)))
+    # every vertex needs an entry: chain the isolated ones to their successor
+    deg = np.bincount(np.array(src, dtype=np.int64), minlength=n) if src else np.zeros(n, int)
+    for u in range(n):
+        if deg[u] == 0:
+            v = (u + 1) % n
+            src += [u, v]
+            dst += [v, u]
+            wts += [1.0, 1.0]
+    order = np.lexsort((np.array(dst), np.array(src)))
+    s = np.array(src, dtype=np.int64)[order]
+    d = np.array(dst, dtype=np.int32)[order]
+    w = np.array(wts, dtype=np.float32)[order]
+    row = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(s, minlength=n), out=row[1:])
+    return CSRGraph(n=n, row_ptr=row, col=d, w=w, name=f"random_{seed}")
+
+
+def test_oracle_refine_equals_restatement_random(oracle):
+    """Many small random graphs (n 3..60, densities 0.05..0.5, integer weights, self-loops),
+    every mode: the oracle's refined partition is the restatement's."""
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    @hyp.settings(max_examples=60, deadline=None, derandomize=True)
+    @hyp.given(seed=st.integers(0, 10**6), n=st.integers(3, 60), p=st.floats(0.05, 0.5),
+               loops=st.booleans(), mode=st.sampled_from([0, 1, 2, 3]))
+    def check(seed, n, p, loops, mode):
+        g = _random_graph(seed, n, p, loops)
+        o = oracle.Oracle(g, mode=mode, refine=True)
+        o.optimization_run()
+        row, col, w = o.graph()
+        labels = R.refine(row.tolist(), col.tolist(), w.tolist(), o.k().tolist(), o.comm().tolist(),
+                          o.totals().tolist(), o.total_weight, mode=mode)
+        o.aggregation_run(True)
+        np.testing.assert_array_equal(o.best(), R.renumber(labels))
+
+    check()
