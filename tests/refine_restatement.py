@@ -1,5 +1,11 @@
-"""A second, independent restatement of the refinement step, in plain Python (test
-infrastructure: it checks the C oracle's refine_partition on small graphs).
+"""A second, independent restatement of the refined pipeline, in plain Python (test
+infrastructure: it checks the C oracle's refine_partition and its refined level loop on small
+graphs). `refine` is the refinement step; `louvain_refined` the whole run: the reference's
+passes (fast pass with the v <= c gate, SORT / HASH tie rules, synchronous moves, the active
+set), the refinement, aggregation by the refined partition, the continuation rule (a smaller
+aggregate and either a gain above the threshold since the previous level's end or fewer than
+tolerance x n refined communities) and the return to the previous level's partition when the
+last level ends below it.
 
 Leiden's RefinePartition / MergeNodesSubset (Traag, Waltman, van Eck 2019, Algorithm A.2) in
 the greedy, pass-synchronous form the engine defines:
@@ -105,3 +111,137 @@ def renumber(labels: np.ndarray) -> np.ndarray:
     """New ids in ascending label order (phaseAggregation.cuh:27-43 on the refined labels)."""
     used = np.unique(labels)
     return np.searchsorted(used, labels)
+
+
+# ---- the whole refined run (small graphs; no edge chunking) ---------------------------------------
+def _gain_self(w_vc: float, self_v: float, k: float, a_own: float, a_c: float, m: float) -> np.float32:
+    diff = np.float32(np.float32(w_vc) - np.float32(self_v))
+    t1 = float(diff) / m
+    t2 = (k * ((a_own - k) - a_c)) / ((2.0 * m) * m)
+    return np.float32(t1 + t2)
+
+
+def _pass(row, col, w, k, comm, a, active, m, mode, it_in_level, fast):
+    """One synchronous pass with the reference's rules; returns the moved flags."""
+    n = len(row) - 1
+    hash_rule = (not fast) and (mode in (0, 3) or (mode == 2 and it_in_level > 4))
+    dec = [-1] * n
+    dg = [np.float32(0.0)] * n
+    for v in range(n):
+        if not active[v] or not any(col[e] != v for e in range(row[v], row[v + 1])):
+            continue
+        cv, kv, a_own = comm[v], k[v], a[comm[v]]
+        bc, bg, have = -1, np.float32(0.0), False
+        if fast:
+            for e in range(row[v], row[v + 1]):
+                u = col[e]
+                if u == v:
+                    continue
+                g = _gain_self(w[e], 0.0, kv, a_own, a[comm[u]], m)
+                if not have or g > bg:
+                    bc, bg, have = comm[u], g, True
+        else:
+            acc = {}
+            for e in range(row[v], row[v + 1]):
+                u = col[e]
+                if u != v:
+                    acc[comm[u]] = acc.get(comm[u], 0.0) + w[e]
+            self_v = float(np.float32(acc[cv])) if cv in acc else 0.0
+            for c in sorted(acc):
+                if hash_rule and c == cv:
+                    continue
+                g = _gain_self(acc[c], self_v, kv, a_own, a[c], m)
+                if hash_rule:
+                    if g > 0 and (not have or g >= bg):
+                        bc, bg, have = c, g, True
+                elif not have or g > bg:
+                    bc, bg, have = c, g, True
+        dec[v], dg[v] = bc, bg
+    moved = [False] * n
+    for v in range(n):
+        c = dec[v]
+        if c < 0 or comm[v] == c or not (dg[v] > 0) or (fast and v > c):
+            continue
+        a[c] += k[v]
+        a[comm[v]] -= k[v]
+        comm[v] = c
+        moved[v] = True
+    for v in range(n):
+        active[v] = any(moved[col[e]] and comm[col[e]] != comm[v] for e in range(row[v], row[v + 1]))
+    return moved
+
+
+def _aggregate(row, col, w, part):
+    """Renumber `part` by ascending label, contract: sorted rows, summed integer weights."""
+    n = len(row) - 1
+    new = renumber(np.array(part))
+    n2 = int(new.max()) + 1
+    rows = [dict() for _ in range(n2)]
+    for v in range(n):
+        r = rows[new[v]]
+        for e in range(row[v], row[v + 1]):
+            d = int(new[col[e]])
+            r[d] = r.get(d, 0) + int(w[e])
+    row2, col2, w2 = [0], [], []
+    for r in rows:
+        for d in sorted(r):
+            col2.append(d)
+            w2.append(r[d])
+        row2.append(len(col2))
+    k2 = [float(sum(w2[row2[s]:row2[s + 1]])) for s in range(n2)]
+    return new, row2, col2, w2, k2
+
+
+def louvain_refined(row, col, w, mode=1, threshold=1e-3, tolerance=0.95, fast_first=True,
+                    max_passes=0, info=None):
+    """Final (best partition per input vertex, modularity) of a refined run; `info` (a dict),
+    if given, receives the number of levels and whether the run returned to the previous
+    level's partition."""
+    row, col, w = list(row), list(col), [int(x) for x in w]
+    n0 = len(row) - 1
+    k = [float(sum(w[row[v]:row[v + 1]])) for v in range(n0)]
+    m = sum(k) / 2.0
+    best = np.arange(n0)
+    prev = None      # per vertex: its members' community at the previous level's end
+    prev_end = 0.0
+    level = 0
+    while True:
+        n = len(row) - 1
+        comm, a, active = list(range(n)), list(k), [True] * n
+        q = _modularity(row, col, w, comm, a, m)
+        start = q
+        it = 0
+        while True:
+            _pass(row, col, w, k, comm, a, active, m, mode, it, fast_first and it == 0)
+            it += 1
+            qn = _modularity(row, col, w, comm, a, m)
+            delta, q = qn - q, qn
+            if not (delta > threshold):
+                break
+        old = prev_end if level > 0 else start
+        cont = (q - old) > threshold
+        prev_end = q
+        labels = refine(row, col, w, k, comm, a, m, mode=mode, threshold=threshold, max_passes=max_passes)
+        n_ref = int(sum(1 for v in range(n) if labels[v] == v))
+        cont = n_ref < n and (cont or n_ref < tolerance * n)
+        if not cont:
+            final = comm
+            reverted = level > 0 and q < old
+            if reverted:
+                final, q = prev, old
+            if info is not None:
+                info["levels"] = level + 1
+                info["reverted"] = reverted
+            ids = renumber(np.array(final))
+            return ids[best], q
+        new, row2, col2, w2, k2 = _aggregate(row, col, w, labels)
+        # each new vertex keeps its members' community, labelled by its smallest new vertex
+        lab = {}
+        for v in range(n):
+            lab[comm[v]] = min(lab.get(comm[v], 1 << 62), int(new[v]))
+        prev = [0] * (int(new.max()) + 1)
+        for v in range(n):
+            prev[int(new[v])] = lab[comm[v]]
+        best = new[best]
+        row, col, w, k = row2, col2, w2, k2
+        level += 1

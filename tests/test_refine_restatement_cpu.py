@@ -102,3 +102,36 @@ def test_oracle_refine_equals_restatement_random(oracle):
         np.testing.assert_array_equal(o.best(), R.renumber(labels))
 
     check()
+
+
+@pytest.mark.parametrize("case", ["chung_lu_1500", "rmat9", "random_a", "random_b"])
+@pytest.mark.parametrize("mode", [1, 0])
+def test_oracle_refined_run_equals_restatement(case, mode, oracle, graphs):
+    """The whole refined run -- passes, refinement, continuation rule, the end-of-run return to
+    the previous level's partition -- in the restatement gives the oracle's final partition and
+    modularity."""
+    g = {"chung_lu_1500": lambda: graphs.chung_lu_bounded(1500, 2.0, 1, 40, seed=3),
+         "rmat9": lambda: graphs.rmat(9, 8, seed=5),
+         "random_a": lambda: _random_graph(11, 60, 0.08, True),
+         "random_b": lambda: _random_graph(12, 80, 0.05, False)}[case]()
+    o = oracle.Oracle(g, mode=mode, refine=True)
+    o.louvain()
+    best, q = R.louvain_refined(g.row_ptr.tolist(), g.col.tolist(), g.weights_or_ones.tolist(), mode=mode)
+    np.testing.assert_array_equal(o.best(), best)
+    assert q == o.modularity
+
+
+@pytest.mark.parametrize("seed,n,p,loops", [(23, 60, 0.06, False), (30, 30, 0.2, True)])
+@pytest.mark.parametrize("mode", [1, 0])
+def test_oracle_refined_run_returns_previous_partition(seed, n, p, loops, mode, oracle):
+    """Graphs whose last level ends below the previous level's end: both return the previous
+    level's partition and its modularity."""
+    g = _random_graph(seed, n, p, loops)
+    info = {}
+    best, q = R.louvain_refined(g.row_ptr.tolist(), g.col.tolist(), g.weights_or_ones.tolist(),
+                                mode=mode, info=info)
+    assert info["reverted"] and info["levels"] >= 2
+    o = oracle.Oracle(g, mode=mode, refine=True)
+    o.louvain()
+    np.testing.assert_array_equal(o.best(), best)
+    assert q == o.modularity
