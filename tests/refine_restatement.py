@@ -245,3 +245,31 @@ def louvain_refined(row, col, w, mode=1, threshold=1e-3, tolerance=0.95, fast_fi
         best = new[best]
         row, col, w, k = row2, col2, w2, k2
         level += 1
+
+
+def louvain_plain(row, col, w, mode=1, threshold=1e-3, fast_first=True):
+    """Final (best partition per input vertex, modularity) of an unrefined run: the level loop
+    of modularityAlgorithms.h:31-67 over the same passes (small graphs, no edge chunking)."""
+    row, col, w = list(row), list(col), [int(x) for x in w]
+    n0 = len(row) - 1
+    k = [float(sum(w[row[v]:row[v + 1]])) for v in range(n0)]
+    m = sum(k) / 2.0
+    best = np.arange(n0)
+    while True:
+        n = len(row) - 1
+        comm, a, active = list(range(n)), list(k), [True] * n
+        q = _modularity(row, col, w, comm, a, m)
+        start = q
+        it = 0
+        while True:
+            _pass(row, col, w, k, comm, a, active, m, mode, it, fast_first and it == 0)
+            it += 1
+            qn = _modularity(row, col, w, comm, a, m)
+            delta, q = qn - q, qn
+            if not (delta > threshold):
+                break
+        new, row2, col2, w2, k2 = _aggregate(row, col, w, comm)
+        best = new[best]
+        if not (q - start) > threshold:
+            return best, q
+        row, col, w, k = row2, col2, w2, k2

@@ -135,3 +135,24 @@ def test_oracle_refined_run_returns_previous_partition(seed, n, p, loops, mode, 
     o.louvain()
     np.testing.assert_array_equal(o.best(), best)
     assert q == o.modularity
+
+
+def test_oracle_plain_run_equals_restatement_random(oracle):
+    """The unrefined run too, on random small graphs in every mode: the restatement's final
+    partition and modularity are the oracle's (which the reference's own goldens pin)."""
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    @hyp.settings(max_examples=40, deadline=None, derandomize=True)
+    @hyp.given(seed=st.integers(0, 10**6), n=st.integers(3, 60), p=st.floats(0.05, 0.5),
+               loops=st.booleans(), mode=st.sampled_from([0, 1, 2, 3]), fast=st.booleans())
+    def check(seed, n, p, loops, mode, fast):
+        g = _random_graph(seed, n, p, loops)
+        o = oracle.Oracle(g, mode=mode, fast_first=fast)
+        o.louvain()
+        best, q = R.louvain_plain(g.row_ptr.tolist(), g.col.tolist(), g.weights_or_ones.tolist(),
+                                  mode=mode, fast_first=fast)
+        np.testing.assert_array_equal(o.best(), best)
+        assert q == o.modularity
+
+    check()
