@@ -16,7 +16,7 @@
 //
 // The passes reuse the optimisation kernels unchanged. They run through a second Dev (the
 // "refine view") in which the graph is the level restricted to entries inside a community
-// (rows in rowB/colB/wB, built by k_ref_count + scan + k_ref_fill), the partition is ref /
+// (rows in rowB/colB/wB, built by k_ref_count[_long] + scan + k_ref_fill[_long]), the partition is ref /
 // ref_new, the totals aref and the graph states gsR. So a singleton's candidates are exactly
 // the refined communities inside its own community, with self = 0 and a_own = k_v. Only the
 // active set (k_ref_select) and the resolution (k_ref_resolve, k_ref_reject) are specific.
