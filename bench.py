@@ -383,8 +383,13 @@ def run_served(args, local):
     with ClockSampler(local) as clk:
         for rate in [float(x) for x in args.rates.split(",")]:
             n_req = int(min(400, max(24, rate * 2.0)))
+            if n_req >= len(pool):
+                # whole shuffled cycles of the pool: the same request mix as the loop baseline
+                n_req = -(-n_req // len(pool)) * len(pool)
+                which = np.concatenate([rng.permutation(len(pool)) for _ in range(n_req // len(pool))])
+            else:
+                which = rng.integers(0, len(pool), n_req)
             gaps = rng.exponential(1.0 / rate, n_req)
-            which = rng.integers(0, len(pool), n_req)
             ids, lat = {}, []
             t_start = time.perf_counter()
             t_next = t_start
