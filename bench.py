@@ -53,9 +53,12 @@ def parse():
     ap.add_argument("--mode", default="SORT", choices=["SORT", "HASH"])
     ap.add_argument("--cpu-sample-scale", type=int, default=21)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA build beside the default line")
     ap.add_argument("--once", action="store_true",
                     help="one untimed run on the device-resident graph (for profilers), then exit")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "batched", "served", "ingest"],
+    ap.add_argument("--workload", default="rmat",
+                    choices=["rmat", "batched", "served", "ingest", "planted"],
                     help="rmat: the single R-MAT graph (default line); batched: 4,096 uneven "
                          "Chung-Lu graphs in one batch against a loop of single runs; served: "
                          "Poisson request stream through the server against a loop")
@@ -186,6 +189,15 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def workload_config(args, g):
+    """The `config` object of both arms' lines (the same keys and values for the same run)."""
+    csr_gb = (8 * (g.n + 1) + 4 * g.E) / 1e9
+    return {"workload": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "mode": args.mode,
+            "threshold": 1e-3, "refine": bool(args.refine),
+            "l2": f"inputs larger than L2 (CSR {csr_gb:.2f} GB)" if csr_gb > 0.126
+                  else f"inputs smaller than L2 (CSR {csr_gb:.3f} GB)"}
+
+
 def cpu_sample(args):
     """The oracle, single-threaded, on a bounded sample of the workload: an R-MAT graph of
     the same generator at a smaller scale (about 10-30 s of CPU work)."""
@@ -224,8 +236,7 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32+f64",
         "data": "synthetic",
-        "config": {"workload": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "mode": args.mode,
-                   "threshold": 1e-3, "refine": bool(args.refine)},
+        "config": workload_config(args, g),
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "port",
                          "sample": f"the full workload graph per step, oracle/louvain_oracle.c "
                                    f"with {threads} OpenMP threads (the reference has no CPU path)"},
@@ -234,6 +245,55 @@ def run_reference(args, world, rank):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# The scale-22 graph on which the reference's CUDA build was checked to run cleanly: the oracle
+# predicts no overrun of its modularity scratch (community.h:69) and its partition matched the
+# oracle's (tests/golden/reference_summary.json). Other graphs are not given to it here.
+REF_CUDA_SAFE_DIGEST = {22: "40d94c8afc4dc4fc"}
+REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_louvain")
+
+
+def reference_cuda(g, args, runs=2):
+    """The reference's own CUDA build (oracle/_ref/ref_louvain: its unmodified sources driven
+    through ModularityAlgorithms::Louvain) on the same graph and mode, on this GPU: its own timed
+    window (modularityAlgorithms.h:26,69-75, the `Total Execution Time` it prints) and the
+    call time around Louvain() (ref_driver.cu: the window plus Community's upload and device
+    graph build). The first run warms the GPU and the file cache and is not reported."""
+    import hashlib
+    import re
+    import tempfile
+    if not os.path.exists(REF_CUDA_BIN):
+        return {"unavailable": "oracle/_ref/ref_louvain not built (make -C oracle ref REF=<tree>)"}
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(g.row_ptr, dtype=np.int64).tobytes())
+    h.update(np.ascontiguousarray(g.col, dtype=np.int32).tobytes())
+    if REF_CUDA_SAFE_DIGEST.get(args.scale) != h.hexdigest()[:16]:
+        return {"unavailable": f"scale {args.scale}: graph not among those checked to run cleanly "
+                               "on the reference's CUDA build"}
+    with tempfile.TemporaryDirectory() as d:
+        inp, out = os.path.join(d, "graph.csr"), os.path.join(d, "res.bin")
+        with open(inp, "wb") as f:
+            np.array([g.n, g.E], dtype=np.int64).tofile(f)
+            np.ascontiguousarray(g.row_ptr, dtype=np.int64).tofile(f)
+            np.ascontiguousarray(g.col, dtype=np.int32).tofile(f)
+        recs = []
+        for _ in range(runs):
+            p = subprocess.run([REF_CUDA_BIN, inp, args.mode, out, "csr"], capture_output=True,
+                               text=True, timeout=600)
+            if p.returncode != 0:
+                return {"unavailable": f"reference exited {p.returncode}: {p.stderr[-300:]}"}
+            t = re.search(r"Total Execution Time: ([0-9.eE+-]+)ms", p.stdout)
+            with open(out, "rb") as f:
+                _, nb = np.frombuffer(f.read(8), dtype=np.uint32)
+                q = float(np.frombuffer(f.read(8), dtype=np.float64)[0])
+                call_ms = float(np.frombuffer(f.read(4), dtype=np.float32)[0])
+            recs.append({"window_ms": float(t.group(1)) if t else None, "call_ms": call_ms,
+                         "modularity": q, "n_communities": int(nb)})
+    r = recs[-1]
+    r.update({"mode": args.mode, "runs": runs, "reported": "last run (the first warms up)",
+              "binary": "oracle/_ref/ref_louvain (reference sources, nvcc -O3 sm_100a)"})
+    return r
 
 
 def run_batched(args, local):
@@ -488,6 +548,86 @@ def run_ingest(args, local):
     return 0
 
 
+def run_planted(args, local):
+    """The planted-partition workload: 1,000,000 vertices in 1,000 power-law-sized communities
+    (exponent 1.5, sizes in [100, 5000]), mean degree 20, mu = 0.3, fp32 weights U[0.5, 1.5]
+    inside and U[0.1, 0.5] between communities, seed 1 (graphs.planted_partition). One step =
+    one complete Louvain run; value = m / device seconds with the CSR resident in HBM, e2e the
+    same through the C ABI from pinned host buffers. The result's NMI against the planted
+    truth is reported; the reference cannot read weights, so its CPU arm is the oracle."""
+    import importlib
+    import torch
+    lv = importlib.import_module(PKG)
+    graphs = importlib.import_module(PKG + ".graphs")
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    g = graphs.planted_partition(n=1_000_000, n_comm=1000, exponent=1.5, smin=100, smax=5000,
+                                 mean_degree=20.0, mu=0.3, seed=1)
+    mode = lv.MODE.SORT if args.mode == "SORT" else lv.MODE.HASH
+    eng = lv.Engine(local, mode=mode)
+    row_d = torch.from_numpy(g.row_ptr).to(dev)
+    col_d = torch.from_numpy(g.col).to(dev)
+    w_d = torch.from_numpy(g.w).to(dev)
+    out_d = torch.empty(g.n, dtype=torch.int32, device=dev)
+    row_h = torch.from_numpy(g.row_ptr).pin_memory().numpy()
+    col_h = torch.from_numpy(g.col).pin_memory().numpy()
+    w_h = torch.from_numpy(g.w).pin_memory().numpy()
+    out_h = torch.empty(g.n, dtype=torch.int32).pin_memory().numpy()
+    clk = ClockSampler(local).__enter__()
+    for _ in range(args.warmup):
+        eng.run_csr(g.n, row_d, col_d, w_d, out=out_d)
+    torch.cuda.synchronize()
+    clk.mark()
+    stats = []
+    for _ in range(args.steps):
+        _, q, st = eng.run_csr(g.n, row_d, col_d, w_d, out=out_d)
+        stats.append(st)
+    torch.cuda.synchronize()
+    ms = sum(s_.ms_total for s_ in stats) / len(stats)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        best, q_e2e, _ = eng.run_csr(g.n, row_h, col_h, w_h, out=out_h)
+    e2e_sec = (time.perf_counter() - t0) / args.steps
+    clk.__exit__(None, None, None)
+    st = stats[-1]
+    peak, peak_kind = measured_peak()
+    achieved = st.bytes_optimization / (st.ms_optimization_kernels / 1e3) / 1e9 if st.ms_optimization_kernels > 0 else 0.0
+    line = {
+        "metric": "louvain_edges_per_s", "value": g.m / (ms / 1e3), "unit": "edges/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 weights, f64 sums", "data": "synthetic",
+        "config": {"workload": "planted_n1000000_c1000_mu0.3_weighted", "n": g.n, "m": g.m,
+                   "mode": args.mode, "threshold": 1e-3,
+                   "l2": f"inputs larger than L2 (CSR {(8 * (g.n + 1) + 8 * g.E) / 1e9:.2f} GB)"},
+        "modularity": q, "n_communities": st.n_communities, "levels": st.levels,
+        "passes": st.iterations, "nmi_vs_truth": graphs.nmi(best, g.truth),
+        "truth_communities": int(np.unique(g.truth).size),
+        "e2e": {"value": g.m / e2e_sec, "unit": "edges/s",
+                "h2d_bytes_per_step": int(g.row_ptr.nbytes + g.col.nbytes + g.w.nbytes),
+                "d2h_bytes_per_step": int(g.n * 4), "ms_per_step": e2e_sec * 1e3, "modularity": q_e2e},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "kernel": "optimisation kernels, all passes",
+                     "bytes": st.bytes_optimization, "ms": st.ms_optimization_kernels,
+                     "peak_source": peak_kind},
+        "clocks": clk.summary(),
+        "gpu_launches": int(sum(s_.kernel_launches for s_ in stats)),
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        o = O.Oracle(g, mode=O.SORT if args.mode == "SORT" else O.HASH, nthreads=1)
+        o.louvain()
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": g.m / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+                                "sample": f"the same graph, one full run, oracle/louvain_oracle.c, "
+                                          f"1 thread, {dt:.2f} s"}
+        line["oracle_same_partition"] = bool(np.array_equal(best, o.best()))
+    print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
@@ -503,6 +643,8 @@ def main():
         return run_served(args, local) if rank == 0 else 0
     if args.workload == "ingest":
         return run_ingest(args, local) if rank == 0 else 0
+    if args.workload == "planted":
+        return run_planted(args, local) if rank == 0 else 0
 
     import importlib
     import torch
@@ -586,10 +728,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 weights, f32 gains, f64 totals", "data": "synthetic",
-        "config": {"workload": f"rmat_s{args.scale}_ef16", "n": g.n, "m": g.m, "mode": args.mode,
-                   "threshold": 1e-3, "refine": bool(args.refine),
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (CSR 1.03 GB)"},
+        "config": workload_config(args, g),
+        "parallelism": "replicas" if world > 1 else "single",
         "modularity": q, "n_communities": st.n_communities, "levels": st.levels,
         "passes": st.iterations, "refine_passes": st.refine_passes,
         "window_ms": st.ms_window, "optimization_ms": st.ms_optimization,
@@ -609,6 +749,15 @@ def main():
         "gpu_launches": int(sum(s.kernel_launches for s in stats)),
         "autotune": tune,
     }
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        rc = reference_cuda(g, args)
+        if rc.get("window_ms"):
+            rc["ours_window_ms"] = st.ms_window
+            rc["ours_e2e_ms"] = e2e_sec * 1e3
+            rc["speedup_window"] = rc["window_ms"] / st.ms_window
+            rc["speedup_e2e_vs_call"] = rc["call_ms"] / (e2e_sec * 1e3)
+            rc["same_modularity"] = abs(rc["modularity"] - q) <= 1e-6
+        line["reference_cuda"] = rc
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args)
     if rank == 0:

@@ -244,11 +244,15 @@ lv_status lv_community_get_trace(lv_community* c, lv_trace_record* out, int32_t 
  * and one scratch array compiled into the library (LV_NOALLOC_MAX_VERTICES + 64 words of 8
  * bytes, held on each GPU that loads the library until the process exits); n above
  * LV_NOALLOC_MAX_VERTICES returns LV_ERR_RANGE before anything runs. Writes out[0..3] =
- * {Q, I, S, m} (device memory; Q is NaN if a label is out of range) asynchronously on
- * `stream` (a cudaStream_t, NULL = default stream). The first call on a device looks up the
- * scratch array's address; make it before any stream capture. Calls that overlap on the GPU
- * share the scratch array and race. weights_integer != 0 (or w == NULL) sums exactly in u64
- * like LV_WEIGHTS_INTEGER; otherwise in double. */
+ * {Q, I, S, m} (device memory) asynchronously on `stream` (a cudaStream_t, NULL = default
+ * stream). Checked on the device: a label or column outside [0, n), or with integer weights a
+ * total weight 2m >= 2^32, makes Q and m NaN; weights summing to zero give m = 0 and Q NaN.
+ * The first call on a device loads this entry point's module (CUDA loads modules lazily),
+ * which reserves the scratch array and the kernels' code in device memory at that moment,
+ * and looks up the array's address: make it before the caller's own pool claims the rest of
+ * HBM and before any stream capture on that device. Calls that overlap on the GPU share the
+ * scratch array and race. weights_integer != 0 (or w == NULL) sums exactly in u64 like
+ * LV_WEIGHTS_INTEGER; otherwise in double. */
 #define LV_NOALLOC_MAX_VERTICES 1048576
 lv_status lv_modularity_noalloc(int64_t n, const int64_t* row_ptr, const int32_t* col, const float* w,
                                 const int32_t* comm, int32_t weights_integer, double* out, void* stream);

@@ -84,6 +84,7 @@ struct Ctrl {
   uint32_t err;
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
+  uint32_t unit_w;             // integer mode, level 0: every weight is 1, so no kernel loads w
   uint32_t bin_count[kNumBins];
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
@@ -242,6 +243,29 @@ __device__ __forceinline__ bool table_add(uint32_t* keys, Acc* vals, uint32_t ma
   return false;
 }
 
+// The same insert, also telling where the key sits and whether this call created it:
+// 0 = no free slot within the probe bound, 1 = the key was there, 2 = this call created it.
+template <class Acc>
+__device__ __forceinline__ int table_add_at(uint32_t* keys, Acc* vals, uint32_t mask, uint32_t shift,
+                                            uint32_t c, Acc w, uint32_t& slot) {
+  uint32_t h = hash_slot(c, shift);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    uint32_t cur = ((volatile uint32_t*)keys)[h];
+    int made = 1;
+    if (cur == kEmpty) {
+      cur = atomicCAS(&keys[h], kEmpty, c);
+      if (cur == kEmpty) { cur = c; made = 2; }
+    }
+    if (cur == c) {
+      acc_add(&vals[h], w);
+      slot = h;
+      return made;
+    }
+    h = (h + 1) & mask;
+  }
+  return 0;
+}
+
 template <class Acc>
 __device__ __forceinline__ Acc table_get(const uint32_t* keys, const Acc* vals, uint32_t mask,
                                          uint32_t shift, uint32_t c) {
@@ -302,6 +326,26 @@ struct PackedTable {
     k = (uint32_t)(x >> 32);
     v = (uint32_t)x;
   }
+  // add() that reports the slot and whether this call created the key (as table_add_at)
+  __device__ __forceinline__ int add_at(uint32_t c, uint32_t w, uint32_t& slot) const {
+    uint32_t h = hash_slot(c, shift);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      unsigned long long cur = ((volatile unsigned long long*)slots)[h];
+      uint32_t key = (uint32_t)(cur >> 32);
+      if (key == kEmpty) {
+        cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
+        if (cur == kEmptySlot) { slot = h; return 2; }
+        key = (uint32_t)(cur >> 32);
+      }
+      if (key == c) {
+        atomicAdd(&slots[h], (unsigned long long)w);
+        slot = h;
+        return 1;
+      }
+      h = (h + 1) & mask;
+    }
+    return 0;
+  }
 };
 
 // A shared-memory table in the layout of the weight mode: packed slots for integer weights,
@@ -324,6 +368,10 @@ struct ScratchTable {
   __device__ __forceinline__ bool add(uint32_t c, Acc w) const {
     if constexpr (WINT) return PackedTable{slots, mask, shift}.add(c, w);
     else return table_add(keys, vals, mask, shift, c, w);
+  }
+  __device__ __forceinline__ int add_at(uint32_t c, Acc w, uint32_t& slot) const {
+    if constexpr (WINT) return PackedTable{slots, mask, shift}.add_at(c, w, slot);
+    else return table_add_at(keys, vals, mask, shift, c, w, slot);
   }
   __device__ __forceinline__ void load(uint32_t i, uint32_t& k, Acc& v) const {
     if constexpr (WINT) {

@@ -120,11 +120,14 @@ struct lv_context {
     pool.emplace(bytes, p);
     pool_bytes += bytes;
   }
+  // Every pooled block came from cudaMallocAsync: freed stream-ordered on the null stream,
+  // then the device is synchronised so that the memory is really back before a retry.
   void drain_pool() {
     std::lock_guard<std::mutex> lk(pool_mu);
-    for (auto& kv : pool) cudaFree(kv.second);
+    for (auto& kv : pool) cudaFreeAsync(kv.second, nullptr);
     pool.clear();
     pool_bytes = 0;
+    cudaDeviceSynchronize();
   }
   bool pool_empty() {
     std::lock_guard<std::mutex> lk(pool_mu);
@@ -174,19 +177,22 @@ struct Block {
 };
 
 // Device allocation through the context's pool; blocks go back to the pool when the run ends.
+// A miss allocates from the device's stream-ordered pool on the run's stream (cudaMallocAsync):
+// unlike cudaMalloc it does not synchronise the device, so a serving slot that meets a new
+// size does not stall the batches running on the other slots' streams.
 template <class T>
-static T* dalloc(lv_context* ctx, std::vector<Block>& owned, size_t count) {
+static T* dalloc(lv_context* ctx, std::vector<Block>& owned, size_t count, cudaStream_t st) {
   if (count == 0) count = 1;
   const size_t bytes = ((count * sizeof(T) + 255) / 256) * 256;
   size_t got = bytes;
   void* p = ctx->take(bytes, &got);
   if (!p) {
     got = bytes;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
     if (e == cudaErrorMemoryAllocation && !ctx->pool_empty()) {
       cudaGetLastError();
       ctx->drain_pool();
-      e = cudaMalloc(&p, bytes);
+      e = cudaMallocAsync(&p, bytes, st);
     }
     LV_CUDA(e);
   }
@@ -330,7 +336,7 @@ class Run {
       if (bins.maxdeg[b + 1] < bins.maxdeg[b]) throw Fail{LV_ERR_ARGUMENT, "bin_max_degree must be non-decreasing"};
     for (int b = 0; b < 6; ++b) team_cap[b] = next_pow2(2u * std::max(1u, bins.maxdeg[b]));
     block_cap = next_pow2(2u * std::max(1u, bins.maxdeg[6]));
-    const size_t slot = 4 + acc_size();
+    const size_t slot = opt_slot_bytes();  // the gain kernels' tables are the larger ones
     int max_smem = 0;
     LV_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     if ((size_t)block_cap * slot > (size_t)max_smem - 1024)
@@ -340,12 +346,18 @@ class Run {
         throw Fail{LV_ERR_ARGUMENT, "team bin table does not fit shared memory"};
   }
 
+  // Shared memory per table slot: the contraction's tables (key + sum) and the gain kernels'
+  // (key + sum, plus half a u32 of key list per slot: the list holds cap / 2 slot indices).
+  size_t con_slot_bytes() const { return 4 + acc_size(); }
+  size_t opt_slot_bytes() const { return 4 + acc_size() + 2; }
+
   template <int T>
   void team_grid(int b, const void* opt_fn, const void* con_fn) {
-    const size_t smem = (size_t)(256 / T) * team_cap[b] * (4 + acc_size());
-    ensure_dyn_smem(ctx->device, opt_fn, smem);
-    ensure_dyn_smem(ctx->device, con_fn, smem);
-    grid_team[b] = ctx->sms * std::max(1, occupancy(ctx->device, opt_fn, 256, smem));
+    const size_t osmem = (size_t)(256 / T) * team_cap[b] * opt_slot_bytes();
+    const size_t csmem = (size_t)(256 / T) * team_cap[b] * con_slot_bytes();
+    ensure_dyn_smem(ctx->device, opt_fn, osmem);
+    ensure_dyn_smem(ctx->device, con_fn, csmem);
+    grid_team[b] = ctx->sms * std::max(1, occupancy(ctx->device, opt_fn, 256, osmem));
   }
 
   template <bool WI>
@@ -356,9 +368,9 @@ class Run {
     team_grid<32>(3, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     team_grid<32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
-    const size_t bsmem = (size_t)block_cap * (4 + acc_size());
+    const size_t bsmem = (size_t)block_cap * opt_slot_bytes();
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
-    ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, bsmem);
+    ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, (size_t)block_cap * con_slot_bytes());
     grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI>, 512, bsmem));
   }
 
@@ -397,7 +409,7 @@ class Run {
     LV_CUDA(cudaMemcpyAsync(row64(), row_ptr, (size_t)(n + 1) * 8, kin, st));
     long long* doffs = nullptr;
     if (G > 1) {
-      doffs = dalloc<long long>(ctx, owned, (size_t)G + 1);
+      doffs = dalloc<long long>(ctx, owned, (size_t)G + 1, st);
       LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
     }
     prepare(ho, doffs, w != nullptr);
@@ -471,7 +483,7 @@ class Run {
       LV_CUDA(cudaMemcpyAsync(D.col + eo[g], ps[g].col, (size_t)ps[g].E * 4, cudaMemcpyHostToDevice, st));
       LV_CUDA(cudaMemcpyAsync(r64 + ho[g], ps[g].row, (size_t)ps[g].n * 8, cudaMemcpyHostToDevice, st));
     }
-    long long* doffs = dalloc<long long>(ctx, owned, 2 * ((size_t)G + 1));
+    long long* doffs = dalloc<long long>(ctx, owned, 2 * ((size_t)G + 1), st);
     LV_CUDA(cudaMemcpyAsync(doffs, ho.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
     LV_CUDA(cudaMemcpyAsync(doffs + G + 1, eo.data(), (G + 1) * 8, cudaMemcpyHostToDevice, st));
     k_rebase_pieces<<<ctx->sms * 4, 256, 0, st>>>(r64, D.col, doffs, doffs + G + 1, G, n, E);
@@ -498,52 +510,52 @@ class Run {
     }
     for (auto& e : ev) LV_CUDA(cudaEventCreate(&e));
     // device arrays (level-0 sizes, reused by every level)
-    D.row = dalloc<uint32_t>(ctx, owned, n + 1);
-    D.rowB = dalloc<uint32_t>(ctx, owned, n + 1);
-    D.col = dalloc<uint32_t>(ctx, owned, E);
-    D.colB = dalloc<uint32_t>(ctx, owned, E);
-    D.w = dalloc<uint32_t>(ctx, owned, E);
-    D.wB = dalloc<uint32_t>(ctx, owned, E);
-    D.k = dalloc<double>(ctx, owned, n);
-    D.kB = dalloc<double>(ctx, owned, n);
-    D.comm = dalloc<uint32_t>(ctx, owned, n);
-    D.a = dalloc<double>(ctx, owned, n);
-    D.new_comm = dalloc<uint32_t>(ctx, owned, n);
-    D.active_it = dalloc<uint32_t>(ctx, owned, n);
-    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n);
-    D.hub_off = dalloc<uint32_t>(ctx, owned, n);
-    D.hubtab = dalloc<uint32_t>(ctx, owned, n);
-    D.hubself = dalloc<unsigned long long>(ctx, owned, n);
-    D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / std::min(kHubPiece, kHubInsPiece) + 16);
-    D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16);
-    D.movers = dalloc<uint32_t>(ctx, owned, n);
-    D.cn = dalloc<unsigned long long>(ctx, owned, n);
-    D.gs = dalloc<GraphState>(ctx, owned, G);
-    D.ctrl = dalloc<Ctrl>(ctx, owned, 1);
-    D.partials = dalloc<double>(ctx, owned, kMaxPartials);
-    D.map = dalloc<unsigned long long>(ctx, owned, n);
-    D.cd = dalloc<unsigned long long>(ctx, owned, (size_t)n + 1);
-    D.rank = dalloc<uint32_t>(ctx, owned, n);
-    D.members = dalloc<uint32_t>(ctx, owned, n);
-    D.newdeg = dalloc<uint32_t>(ctx, owned, (size_t)n + 1);
-    D.best = dalloc<uint32_t>(ctx, owned, n0);
-    D.out = dalloc<int32_t>(ctx, owned, n0);
+    D.row = dalloc<uint32_t>(ctx, owned, n + 1, st);
+    D.rowB = dalloc<uint32_t>(ctx, owned, n + 1, st);
+    D.col = dalloc<uint32_t>(ctx, owned, E, st);
+    D.colB = dalloc<uint32_t>(ctx, owned, E, st);
+    D.w = dalloc<uint32_t>(ctx, owned, E, st);
+    D.wB = dalloc<uint32_t>(ctx, owned, E, st);
+    D.k = dalloc<double>(ctx, owned, n, st);
+    D.kB = dalloc<double>(ctx, owned, n, st);
+    D.comm = dalloc<uint32_t>(ctx, owned, n, st);
+    D.a = dalloc<double>(ctx, owned, n, st);
+    D.new_comm = dalloc<uint32_t>(ctx, owned, n, st);
+    D.active_it = dalloc<uint32_t>(ctx, owned, n, st);
+    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n, st);
+    D.hub_off = dalloc<uint32_t>(ctx, owned, n, st);
+    D.hubtab = dalloc<uint32_t>(ctx, owned, n, st);
+    D.hubself = dalloc<unsigned long long>(ctx, owned, n, st);
+    D.long_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / std::min(kHubPiece, kHubInsPiece) + 16, st);
+    D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16, st);
+    D.movers = dalloc<uint32_t>(ctx, owned, n, st);
+    D.cn = dalloc<unsigned long long>(ctx, owned, n, st);
+    D.gs = dalloc<GraphState>(ctx, owned, G, st);
+    D.ctrl = dalloc<Ctrl>(ctx, owned, 1, st);
+    D.partials = dalloc<double>(ctx, owned, kMaxPartials, st);
+    D.map = dalloc<unsigned long long>(ctx, owned, n, st);
+    D.cd = dalloc<unsigned long long>(ctx, owned, (size_t)n + 1, st);
+    D.rank = dalloc<uint32_t>(ctx, owned, n, st);
+    D.members = dalloc<uint32_t>(ctx, owned, n, st);
+    D.newdeg = dalloc<uint32_t>(ctx, owned, (size_t)n + 1, st);
+    D.best = dalloc<uint32_t>(ctx, owned, n0, st);
+    D.out = dalloc<int32_t>(ctx, owned, n0, st);
     if (G > 1) {
-      D.gid = dalloc<uint32_t>(ctx, owned, n);
-      D.gidB = dalloc<uint32_t>(ctx, owned, n);
-      D.gid0 = dalloc<uint32_t>(ctx, owned, n0);
+      D.gid = dalloc<uint32_t>(ctx, owned, n, st);
+      D.gidB = dalloc<uint32_t>(ctx, owned, n, st);
+      D.gid0 = dalloc<uint32_t>(ctx, owned, n0, st);
     }
-    D.scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2);
+    D.scan_tmp = dalloc<unsigned long long>(ctx, owned, (size_t)(n + 1) / kScanTile + 2, st);
     if (cfg.refine) {
-      D.ref = dalloc<uint32_t>(ctx, owned, n);
-      D.ref_new = dalloc<uint32_t>(ctx, owned, n);
-      D.aref = dalloc<double>(ctx, owned, n);
-      D.rsz = dalloc<uint32_t>(ctx, owned, n);
-      D.rflag = dalloc<uint32_t>(ctx, owned, n);
-      D.gsR = dalloc<GraphState>(ctx, owned, G);
-      D.coarse = dalloc<uint32_t>(ctx, owned, n);
-      D.lab = dalloc<uint32_t>(ctx, owned, n);
-      D.prev = dalloc<uint32_t>(ctx, owned, n);
+      D.ref = dalloc<uint32_t>(ctx, owned, n, st);
+      D.ref_new = dalloc<uint32_t>(ctx, owned, n, st);
+      D.aref = dalloc<double>(ctx, owned, n, st);
+      D.rsz = dalloc<uint32_t>(ctx, owned, n, st);
+      D.rflag = dalloc<uint32_t>(ctx, owned, n, st);
+      D.gsR = dalloc<GraphState>(ctx, owned, G, st);
+      D.coarse = dalloc<uint32_t>(ctx, owned, n, st);
+      D.lab = dalloc<uint32_t>(ctx, owned, n, st);
+      D.prev = dalloc<uint32_t>(ctx, owned, n, st);
     }
     dev_dirty = true;
     bind();
@@ -583,6 +595,7 @@ class Run {
     hc.n = n; hc.E = E; hc.n0 = n0; hc.G = G;
     hc.max_iterations = (uint32_t)std::max(0, cfg.max_iterations);
     hc.threshold = cfg.threshold;
+    hc.unit_w = wint ? 1u : 0u;  // k_prep clears it at the first weight other than 1
     LV_CUDA(cudaMemcpyAsync(D.ctrl, &hc, offsetof(Ctrl, trace), cudaMemcpyHostToDevice, st));
     std::vector<GraphState> hs(G);
     for (uint32_t g = 0; g < G; ++g) {
@@ -648,9 +661,9 @@ class Run {
     }
     uint64_t slots = std::max<uint64_t>(need_slots + need_slots / 4, 1 << 16);
     slots = std::min<uint64_t>(slots, 0xFFFFFFFEull);
-    D.arena_keys = dalloc<uint32_t>(ctx, arena_blocks, slots);
-    D.arena_vals = dalloc<unsigned long long>(ctx, arena_blocks, slots);
-    D.hub_owner = dalloc<uint32_t>(ctx, arena_blocks, slots / kHubChunk + 1);
+    D.arena_keys = dalloc<uint32_t>(ctx, arena_blocks, slots, st);
+    D.arena_vals = dalloc<unsigned long long>(ctx, arena_blocks, slots, st);
+    D.hub_owner = dalloc<uint32_t>(ctx, arena_blocks, slots / kHubChunk + 1, st);
     arena_slots = slots;
     dev_dirty = true;
     bind();
@@ -679,7 +692,7 @@ class Run {
   // ---- one optimisation pass --------------------------------------------------------------------
   template <bool WI>
   void launch_pass(bool view = false) {
-    const size_t slot = 4 + (WI ? 4 : 8);
+    const size_t slot = opt_slot_bytes();
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
     k_chunk_flags<<<grid_n, 256, 0, st>>>(Dd);
     k_bin_vertices<<<grid_n, 256, 0, st>>>(Dd, bins);
@@ -1580,7 +1593,13 @@ lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offs
         for (int b = 0; b < 7; ++b) r.cfg.bin_max_degree[b] = kTuneCandidates[c][b];
         r.cfg.bin_max_degree[7] = 0;
         LV_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
-        r.init((uint32_t)n_graphs, n_graphs > 1 ? vtx_offsets : nullptr, n, row_ptr, col, w, in_mem);
+        try {
+          r.init((uint32_t)n_graphs, n_graphs > 1 ? vtx_offsets : nullptr, n, row_ptr, col, w, in_mem);
+        } catch (const lv::Fail& e) {
+          // a candidate whose tables do not fit shared memory in this weight mode is skipped
+          if (e.st != LV_ERR_ARGUMENT || c == 0) throw;
+          break;
+        }
         r.louvain();
         LV_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
         LV_CUDA(cudaEventSynchronize(ctx->ev[1]));

@@ -244,10 +244,18 @@ struct VtxCtx {
   uint32_t rs, re, cv, ng;  // ng: vertices of v's graph at this level
   double kv, a_own, m, two_m2;
   double own_minus_k, inv_m, inv_2m2;  // a_own - k (the reference's first subtraction); bounds
+  bool unit;                // every weight of the level is 1 (Ctrl::unit_w): w is not loaded
 };
 
-__device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v) {
+// Ctrl::unit_w as a kernel reads it once: only integer-mode kernels may take the shortcut.
+template <bool WINT>
+__device__ __forceinline__ bool unit_weights(const Ctrl* C) {
+  return WINT && C->unit_w != 0;
+}
+
+__device__ __forceinline__ VtxCtx load_vtx(const Dev& D, uint32_t v, bool unit = false) {
   VtxCtx x;
+  x.unit = unit;
   x.rs = D.row[v];
   x.re = D.row[v + 1];
   x.cv = D.comm[v];
@@ -291,7 +299,7 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
       const uint32_t ek = e + k * step;
       const bool in = ek < x.re;
       uu[k] = in ? D.col[ek] : v;
-      wf[k] = in ? Tr::w_float(w[ek]) : 0.0f;
+      wf[k] = in ? (x.unit ? 1.0f : Tr::w_float(w[ek])) : 0.0f;
     }
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) au[k] = uu[k] != v ? D.a[uu[k]] : 0.0;
@@ -332,7 +340,7 @@ __device__ __forceinline__ void insert_scan(const Dev& D, const VtxCtx& x, uint3
       const uint32_t ek = e + k * step;
       const bool in = ek < x.re;
       uu[k] = in ? D.col[ek] : v;
-      ww[k] = in ? (Acc)w[ek] : Acc(0);
+      ww[k] = in ? (x.unit ? Acc(1) : (Acc)w[ek]) : Acc(0);
     }
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
@@ -386,6 +394,118 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
   return best;
 }
 
+// Table pass with a key list: the insert half also records, for every community it creates in
+// the table, the slot it sits in, so that the evaluation half reads only those slots (the
+// distinct neighbouring communities) instead of scanning the whole table, and empties only
+// them again -- a table is cleared once when a kernel starts and stays empty between vertices.
+// The list has room for min(d, ng) slots, half the table's capacity.
+//
+// Insert half. The entries of the row are walked in team-uniform steps (every lane of the team
+// takes the same number of steps, lanes past the row's end carry nothing), so the lanes that
+// created a key can agree on their list positions with one ballot per entry batch. `tmask` is
+// the team's lanes within the warp. BLOCK: the team is the whole block; warps take list space
+// from the shared counter *bcount (one atomic per warp and batch), which the caller reads after
+// a barrier. Otherwise the team is part of one warp and the count is returned.
+template <bool WINT, bool BLOCK, class Tbl>
+__device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t lane,
+                                                uint32_t step, unsigned tmask, const Tbl& tbl,
+                                                uint32_t* list, uint32_t* bcount,
+                                                typename WTraits<WINT>::Acc& self_acc, uint32_t& err) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  using Wt = typename Tr::W;
+  const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  const uint32_t lt = lanemask_lt();
+  uint32_t nl = 0;
+  for (uint32_t b = x.rs; b < x.re; b += kBatch * step) {
+    uint32_t uu[kBatch], cc[kBatch];
+    Acc ww[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ek = b + lane + k * step;
+      const bool in = ek < x.re;
+      uu[k] = in ? D.col[ek] : v;
+      ww[k] = in ? (x.unit ? Acc(1) : (Acc)w[ek]) : Acc(0);
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      bool made = false;
+      uint32_t slot = 0;
+      if (cc[k] != kEmpty) {
+        if (cc[k] == x.cv) {
+          self_acc += ww[k];
+        } else {
+          const int r = tbl.add_at(cc[k], ww[k], slot);
+          if (!r) err |= kErrTableFull;
+          made = r == 2;
+        }
+      }
+      const unsigned m = __ballot_sync(tmask, made) & tmask;
+      if (BLOCK) {
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          uint32_t base = 0;
+          if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(bcount, (uint32_t)__popc(m));
+          base = __shfl_sync(kFull, base, leader);
+          if (made) list[base + __popc(m & lt)] = slot;
+        }
+      } else {
+        if (made) list[nl + __popc(m & lt)] = slot;
+        nl += __popc(m);
+      }
+    }
+  }
+  return nl;
+}
+
+// Evaluation half over the listed slots [i0, nl) with stride `step`: best key over the
+// distinct neighbouring communities (as cand_scan), emptying each slot after reading it.
+template <bool WINT, class Tbl>
+__device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxCtx& x, const Tbl& tbl,
+                                                        const uint32_t* list, uint32_t i0, uint32_t nl,
+                                                        uint32_t step, float self_v, bool lowest) {
+  using Tr = WTraits<WINT>;
+  using Acc = typename Tr::Acc;
+  unsigned long long best = 0;
+  float bestg = 0.0f;
+  for (uint32_t i = i0; i < nl; i += kBatch * step) {
+    uint32_t cc[kBatch];
+    Acc vv[kBatch];
+    double ac[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ik = i + k * step;
+      cc[k] = kEmpty;
+      vv[k] = Acc(0);
+      if (ik < nl) {
+        const uint32_t sl = list[ik];
+        tbl.load(sl, cc[k], vv[k]);
+        tbl.clear(sl);
+      }
+      if (cc[k] == x.cv) cc[k] = kEmpty;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (cc[k] == kEmpty) continue;
+      const float diff = __fsub_rn(Tr::to_float(vv[k]), self_v);
+      const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
+      const float hi = gain_upper(diff, p, x.inv_m, x.inv_2m2);
+      if (hi > 0.0f && hi >= bestg) {
+        const float g = gain_exact(diff, p, x.m, x.two_m2);
+        if (g > 0.0f) {
+          const unsigned long long key = argmax_key(g, cc[k], lowest);
+          if (key > best) { best = key; bestg = g; }
+        }
+      }
+    }
+  }
+  return best;
+}
+
 // ---- pass: optimisation, one team of T lanes per vertex -----------------------------------------
 // Fast pass (iteration 0 of a level, phaseOptimizationSort.cu:28-158): per-entry gains with
 // self = 0 and the destination's own (singleton) community, argmax over positive gains with
@@ -401,56 +521,55 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
-  using Wt = typename Tr::W;
   constexpr int TEAMS = 256 / T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int team = threadIdx.x / T, lane = threadIdx.x % T;
+  // per team: a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 slots
+  constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
+  unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
+  uint32_t* list = reinterpret_cast<uint32_t*>(smem + (size_t)TEAMS * cap * kSlotBytes) + (size_t)team * (cap / 2);
 
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
-  const uint32_t* list = D.bins[bin];
+  if (blockIdx.x * TEAMS >= count) return;  // (block-uniform)
+  const uint32_t* vlist = D.bins[bin];
   const uint32_t it = C->it;
   const bool fast = C->fast != 0;
   const bool lowest = fast || C->rule_sort != 0;
+  const bool unit = unit_weights<WINT>(C);
+  const unsigned tmask = T == 32 ? kFull : (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(uint32_t)(T - 1)));
   uint32_t err = 0;
+  ScratchTable<WINT> tbl{keys, vals, slots, cap - 1u, 0u};
+  if (!fast) {
+    for (uint32_t s = lane; s < cap; s += T) tbl.clear(s);
+    __syncwarp();
+  }
 
   for (uint32_t base = blockIdx.x * TEAMS; base < count; base += gridDim.x * TEAMS) {
     const uint32_t idx = base + team;
     const bool live = idx < count;
-    const uint32_t v = live ? list[idx] : 0u;
+    const uint32_t v = live ? vlist[idx] : 0u;
     VtxCtx x{};
-    if (live) x = load_vtx(D, v);
+    if (live) x = load_vtx(D, v, unit);
     unsigned long long best = 0;
     if (fast) {
       if (live) best = fast_scan<WINT>(D, x, v, x.rs + lane, T);
       best = team_max<T>(best, kFull);
     } else {
       const uint32_t cap_v = live ? table_cap(x.re - x.rs, x.ng) : 2u;
-      const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
+      tbl.mask = cap_v - 1u;
+      tbl.shift = 32u - log2_pow2(cap_v);
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
-      auto table_pass = [&](const auto& tbl) {
-        __syncwarp();
-        if (live) insert_scan<WINT>(D, x, v, x.rs + lane, T, tbl, self_acc, err);
-        self_acc = team_sum<T>(self_acc);
-        __syncwarp();
-        if (live) best = cand_scan<WINT>(D, x, tbl, lane, cap_v, T, Tr::to_float(self_acc), lowest);
-      };
-      if constexpr (WINT) {
-        // integer weights: packed (community << 32 | sum) slots, 8 bytes like the split pair
-        unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
-        if (live)
-          for (uint32_t s = lane; s < cap_v; s += T) slots[s] = kEmptySlot;
-        table_pass(PackedTable{slots, mask, shift});
-      } else {
-        if (live)
-          for (uint32_t s = lane; s < cap_v; s += T) { keys[s] = kEmpty; vals[s] = Acc(0); }
-        table_pass(SplitTable<Acc>{keys, vals, mask, shift});
-      }
-      best = team_max<T>(best, kFull);
+      uint32_t nl = 0;
+      if (live) nl = insert_list<WINT, false>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+      self_acc = team_sum<T>(self_acc);
       __syncwarp();
+      if (live) best = list_scan<WINT>(D, x, tbl, list, lane, nl, T, Tr::to_float(self_acc), lowest);
+      best = team_max<T>(best, kFull);
+      __syncwarp();  // the listed slots are empty again before the next vertex inserts
     }
     bool move = false;
     uint32_t c = 0;
@@ -508,48 +627,48 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
-  using Wt = typename Tr::W;
   constexpr int NT = 512;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long red[33];
+  __shared__ uint32_t nlist;
+  // a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 slots
+  constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
+  Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
+  unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
+  uint32_t* list = reinterpret_cast<uint32_t*>(smem + (size_t)cap * kSlotBytes);
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
-  const uint32_t* list = D.bins[bin];
+  if (blockIdx.x >= count) return;  // (block-uniform)
+  const uint32_t* vlist = D.bins[bin];
   const uint32_t it = C->it;
   const bool fast = C->fast != 0;
   const bool lowest = fast || C->rule_sort != 0;
+  const bool unit = unit_weights<WINT>(C);
   uint32_t err = 0;
+  ScratchTable<WINT> tbl{keys, vals, slots, cap - 1u, 0u};
+  if (!fast)
+    for (uint32_t s = threadIdx.x; s < cap; s += NT) tbl.clear(s);
 
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
-    const uint32_t v = list[idx];
-    const VtxCtx x = load_vtx(D, v);
+    const uint32_t v = vlist[idx];
+    const VtxCtx x = load_vtx(D, v, unit);
     unsigned long long best = 0;
     if (fast) {
       best = fast_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT);
     } else {
       const uint32_t cap_v = table_cap(x.re - x.rs, x.ng);
-      const uint32_t mask = cap_v - 1u, shift = 32u - log2_pow2(cap_v);
       const bool ok = cap_v <= cap;
       if (!ok) err |= kErrArena;
+      tbl.mask = cap_v - 1u;
+      tbl.shift = 32u - log2_pow2(cap_v);
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
-      auto table_pass = [&](const auto& tbl) {
-        __syncthreads();
-        if (ok) insert_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT, tbl, self_acc, err);
-        self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));
-        if (ok) best = cand_scan<WINT>(D, x, tbl, threadIdx.x, cap_v, NT, Tr::to_float(self_acc), lowest);
-      };
-      if constexpr (WINT) {
-        unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
-        if (ok)
-          for (uint32_t s = threadIdx.x; s < cap_v; s += NT) slots[s] = kEmptySlot;
-        table_pass(PackedTable{slots, mask, shift});
-      } else {
-        uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
-        Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
-        if (ok)
-          for (uint32_t s = threadIdx.x; s < cap_v; s += NT) { keys[s] = kEmpty; vals[s] = Acc(0); }
-        table_pass(SplitTable<Acc>{keys, vals, mask, shift});
-      }
+      if (threadIdx.x == 0) nlist = 0;
+      __syncthreads();  // the table is empty and the list count zero
+      if (ok) insert_list<WINT, true>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist, self_acc, err);
+      self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));  // (its barriers order the list)
+      const uint32_t nl = nlist;
+      if (ok) best = list_scan<WINT>(D, x, tbl, list, threadIdx.x, nl, NT, Tr::to_float(self_acc), lowest);
     }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best) {
@@ -603,12 +722,13 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
   Ctrl* C = D.ctrl;
   const uint32_t count = C->hub_items;
   const bool fast = C->fast != 0;
+  const bool unit = unit_weights<WINT>(C);
   uint32_t err = 0;
   for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
     const unsigned long long item = D.long_items[i];
     const uint32_t pos = (uint32_t)(item >> 32), piece = (uint32_t)item;
     const uint32_t v = D.bins[kNumBins - 1][pos];
-    VtxCtx x = load_vtx(D, v);
+    VtxCtx x = load_vtx(D, v, unit);
     const uint32_t d = x.re - x.rs;
     const uint32_t pstart = x.rs + piece * kHubPiece;
     x.re = min(x.re, pstart + kHubPiece);
@@ -706,7 +826,7 @@ __global__ void k_opt_hub_decide(int dslot) {
 template <bool WINT>
 __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t old, uint32_t nw,
                                               uint32_t it, uint32_t e0, uint32_t re, uint32_t step,
-                                              long long& di, double& df) {
+                                              bool unit, long long& di, double& df) {
   using Tr = WTraits<WINT>;
   using Wt = typename Tr::W;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
@@ -736,7 +856,7 @@ __device__ __forceinline__ void apply_entries(const Dev& D, uint32_t v, uint32_t
       if (dd) {
         const uint32_t ek = e + k * step;
         const int f = mu ? dd : 2 * dd;
-        if (WINT) di += (long long)f * (long long)w[ek];
+        if (WINT) di += (long long)f * (unit ? 1ll : (long long)w[ek]);
         else df += (double)f * Tr::w_double(w[ek]);
       }
     }
@@ -771,6 +891,7 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
   // the optimisation kernels of this pass ended when the first apply block starts
   if (blockIdx.x == 0 && threadIdx.x == 0) C->t_optk_ns += global_ns() - C->t_pass0;
   const uint32_t count = C->mover_count, it = C->it;
+  const bool unit = unit_weights<WINT>(C);
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -859,7 +980,7 @@ __global__ void __launch_bounds__(256) k_apply(int dslot) {
               gcur = g;
             }
           }
-          if (WINT) di += (long long)f * (long long)w[ee[q]];
+          if (WINT) di += (long long)f * (unit ? 1ll : (long long)w[ee[q]]);
           else df += (double)f * Tr::w_double(w[ee[q]]);
         }
       }
@@ -882,6 +1003,7 @@ __global__ void __launch_bounds__(256) k_apply_long(int dslot) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->long_movers, it = C->it;
+  const bool unit = unit_weights<WINT>(C);
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -891,7 +1013,7 @@ __global__ void __launch_bounds__(256) k_apply_long(int dslot) {
     const uint32_t g = D.gid ? D.gid[v] : 0u;
     long long di = 0;
     double df = 0.0;
-    apply_entries<WINT>(D, v, old, nw, it, D.row[v] + lane, D.row[v + 1], 32, di, df);
+    apply_entries<WINT>(D, v, old, nw, it, D.row[v] + lane, D.row[v + 1], 32, unit, di, df);
     if (WINT) {
       di = warp_sum(di);
       if (lane == 0 && di) atomicAdd(&D.gs[g].I, (unsigned long long)di);
@@ -909,6 +1031,7 @@ __global__ void __launch_bounds__(512) k_apply_hub(int dslot) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t count = C->apply_items, it = C->it;
+  const bool unit = unit_weights<WINT>(C);
   __shared__ long long shi[32];
   __shared__ double shf[32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -927,7 +1050,7 @@ __global__ void __launch_bounds__(512) k_apply_hub(int dslot) {
     double df = 0.0;
     const uint32_t ps = D.row[v] + piece * kHubPiece;
     const uint32_t pe = min(D.row[v + 1], ps + kHubPiece);
-    apply_entries<WINT>(D, v, old, nw, it, ps + threadIdx.x, pe, blockDim.x, di, df);
+    apply_entries<WINT>(D, v, old, nw, it, ps + threadIdx.x, pe, blockDim.x, unit, di, df);
     di = warp_sum(di);
     df = warp_sum(df);
     if (lane == 0) { shi[wid] = di; shf[wid] = df; }
@@ -1192,6 +1315,8 @@ __global__ void k_chunk_bounds(int dslot, unsigned long long step) {
 // GraphDevice(GraphHost&) (graph.cuh:46-99) and the Community constructor (community.h:31-46):
 // k = sum of incident weights, m = total weight / 2 (graph.cu:81). One warp per vertex.
 constexpr uint32_t kPrepLongRow = 4096;
+// k_prep's local marker (never stored in Ctrl::err): a weight other than 1 was seen.
+constexpr uint32_t kErrNotUnit = 1u << 31;
 
 // Validation and weight conversion of entries [e0, re) with stride `step` of row v (graph
 // vertex range [lo, hi)); sums of the row's weights and of its self-loop weights.
@@ -1211,6 +1336,7 @@ __device__ __forceinline__ void prep_entries(const Dev& D, uint32_t v, long long
       if (!wu_in && (!(x >= 1.0f) || x != floorf(x) || x > 4294967040.0f)) { err |= kErrInput; continue; }
       const uint32_t xi = wu_in ? wu_in[e] : (uint32_t)x;
       if (xi == 0u) { err |= kErrInput; continue; }
+      if (xi != 1u) err |= kErrNotUnit;
       reinterpret_cast<uint32_t*>(D.w)[e] = xi;
       ki += xi;
       if (u == v) si += xi;
@@ -1287,6 +1413,8 @@ __global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64,
     }
   }
   flush();
+  if (err & kErrNotUnit) C->unit_w = 0;
+  err &= ~kErrNotUnit;
   if (err) atomicOr(&C->err, err);
 }
 
@@ -1324,6 +1452,8 @@ __global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in
       }
     }
   }
+  if (err & kErrNotUnit) C->unit_w = 0;
+  err &= ~kErrNotUnit;
   if (err) atomicOr(&C->err, err);
 }
 
@@ -2136,6 +2266,7 @@ __global__ void k_agg_finish(int dslot) {
     }
     C->n = n2;
     C->E = C->E_next;
+    C->unit_w = 0;  // contracted weights are sums
     C->seg_levels += 1;
     C->t_agg_ns += global_ns() - C->t_agg0;
   }

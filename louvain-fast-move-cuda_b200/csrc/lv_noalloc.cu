@@ -17,8 +17,18 @@
 //
 // Set-up: host code cannot pass the array's name to a kernel (in host code that name is only a
 // stand-in, not a device address). The first call on each device, with that device current,
-// asks the runtime for the array's device address with cudaGetSymbolAddress and keeps it;
-// make that first call before any stream capture on the device.
+// asks the runtime for the array's device address with cudaGetSymbolAddress and keeps it.
+// Under CUDA's default lazy module loading, that first call is also the moment this file's
+// module is loaded onto the device: the 8 MiB array and the kernels' code are reserved in
+// device memory then, not when the library is opened. So make the first call on each device
+// before the caller's own pool claims the rest of HBM (otherwise it returns LV_ERR_CUDA), and
+// before any stream capture on the device.
+//
+// Input checks happen on the device (the call never synchronises): a label or a column
+// outside [0, n), or, with integer weights, a total weight 2m of 2^32 or more (the sum of
+// squared totals is exact in u64 only below it), makes out[0] (Q) and out[3] (m) NaN. A graph
+// whose weights sum to zero has m = 0 and Q = 0/0: out[0] is NaN and out[3] is 0, so the two
+// cases stay apart.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -48,8 +58,8 @@ __global__ void k_na_clear(unsigned long long* s, uint32_t n) {
 }
 
 // One warp per vertex: k_v, its community's total, the internal weight (entries whose ends
-// share a community, community.h:87-100) and the total weight. Labels outside [0, n) set a
-// flag instead of being used.
+// share a community, community.h:87-100) and the total weight. Labels and columns outside
+// [0, n) set a flag instead of being used.
 template <bool WINT>
 __global__ void k_na_rows(const long long* row, const int32_t* col, const float* w,
                           const int32_t* comm, uint32_t n, unsigned long long* s) {
@@ -64,10 +74,13 @@ __global__ void k_na_rows(const long long* row, const int32_t* col, const float*
     }
     unsigned long long ki = 0, ii = 0;
     double kf = 0.0, iff = 0.0;
+    bool bad_col = false;
     for (long long e = row[v] + lane; e < row[v + 1]; e += 32) {
       const int32_t u = col[e];
       const float x = w ? w[e] : 1.0f;
-      const bool same = u >= 0 && (uint32_t)u < n && comm[u] == cv;
+      const bool in = u >= 0 && (uint32_t)u < n;
+      bad_col |= !in;
+      const bool same = in && comm[u] == cv;
       if (WINT) {
         ki += (unsigned long long)x;
         if (same) ii += (unsigned long long)x;
@@ -83,6 +96,7 @@ __global__ void k_na_rows(const long long* row, const int32_t* col, const float*
       kf += __shfl_xor_sync(0xFFFFFFFFu, kf, o);
       iff += __shfl_xor_sync(0xFFFFFFFFu, iff, o);
     }
+    if (__any_sync(0xFFFFFFFFu, bad_col) && lane == 0) atomicOr(&s[LV_NOALLOC_MAX_VERTICES + 3], 2ull);
     if (lane == 0) {
       if (WINT) {
         atomicAdd(&s[cv], ki);
@@ -129,10 +143,13 @@ __global__ void k_na_result(const unsigned long long* s, double* out) {
     k = __longlong_as_double((long long)acc[2]);
   }
   const double m = k / 2.0;
-  out[0] = acc[3] ? __longlong_as_double(0x7FF8000000000000ll) : dq(I, S, m);  // NaN: bad label
+  // flags: 1 a label out of range, 2 a column out of range, 4 integer total weight 2m >= 2^32
+  const unsigned long long flags = acc[3] | (WINT && acc[2] >= (1ull << 32) ? 4ull : 0ull);
+  const double nan = __longlong_as_double(0x7FF8000000000000ll);
+  out[0] = flags ? nan : dq(I, S, m);  // m = 0 gives 0/0 = NaN with out[3] = 0
   out[1] = I;
   out[2] = S;
-  out[3] = m;
+  out[3] = flags ? nan : m;
 }
 
 }  // namespace

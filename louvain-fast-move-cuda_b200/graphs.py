@@ -221,6 +221,29 @@ def planted_partition(n: int = 1_000_000, n_comm: int = 1000, exponent: float = 
                                 truth=label)
 
 
+def nmi(a: np.ndarray, b: np.ndarray) -> float:
+    """Normalised mutual information of two labelings, I(A;B) / sqrt(H(A) H(B)) in nats
+    (the geometric normalisation); 1.0 when both labelings have a single class."""
+    a = np.unique(np.asarray(a), return_inverse=True)[1].astype(np.int64)
+    b = np.unique(np.asarray(b), return_inverse=True)[1].astype(np.int64)
+    n = a.size
+    if n == 0:
+        return 1.0
+    pair, cnt = np.unique(a * (int(b.max()) + 1) + b, return_counts=True)
+    ca = np.bincount(a).astype(np.float64)
+    cb = np.bincount(b).astype(np.float64)
+    pa, pb = ca / n, cb / n
+    ha = -np.sum(pa * np.log(pa))
+    hb = -np.sum(pb * np.log(pb))
+    pij = cnt / n
+    ia = pair // (int(b.max()) + 1)
+    ib = pair % (int(b.max()) + 1)
+    mi = float(np.sum(pij * (np.log(pij) - np.log(pa[ia]) - np.log(pb[ib]))))
+    if ha <= 0.0 or hb <= 0.0:
+        return 1.0 if ha == hb else 0.0
+    return max(0.0, min(1.0, mi / np.sqrt(ha * hb)))
+
+
 def read_edge_list(path: str, skip_line: int = 0) -> CSRGraph:
     """Parse an unweighted ``a b`` edge list the way the reference's GraphHost does
     (graph.cu:17-87): skip header lines, dedup undirected pairs, emit both directions with

@@ -1,7 +1,8 @@
 """Generate golden vectors by running the reference's own CUDA build.
 
 This is the script that produced the committed fixtures in this directory. It needs a
-CUDA GPU and the reference binary built by ``make -C oracle ref`` (oracle/_ref/ref_louvain,
+CUDA GPU and the reference binary built by ``make -C oracle ref REF=<reference tree>``
+(oracle/_ref/ref_louvain,
 compiled from the reference's unmodified sources). For each case and mode it
 
   1. builds the input graph (the reference's bundled fixture, read from
@@ -15,8 +16,8 @@ compiled from the reference's unmodified sources). For each case and mode it
      own timed window (modularityAlgorithms.h:69-75).
 
 usage:
-  python tests/golden/make_golden.py --out gpurun_out/golden            # parity cases
-  python tests/golden/make_golden.py --out gpurun_out/golden --rmat22   # + scale-22 run
+  python tests/golden/make_golden.py --out <dir>            # parity cases
+  python tests/golden/make_golden.py --out <dir> --rmat22   # + scale-22 run
   python tests/golden/make_golden.py --import-fixture <graph-power-law-10000-2-99-1.edge>
 """
 from __future__ import annotations
@@ -143,7 +144,8 @@ def run_reference(g, mode: str, workdir: str, big: bool = False):
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(tempfile.gettempdir(), "louvain_golden"),
+                    help="directory for the new golden files (copy the ones you keep into tests/golden)")
     ap.add_argument("--rmat22", action="store_true")
     ap.add_argument("--only", default=None)
     ap.add_argument("--import-fixture", default=None)
@@ -152,7 +154,7 @@ def main() -> int:
         import_fixture(a.import_fixture)
         return 0
     if not os.path.exists(REF_BIN):
-        print(f"missing {REF_BIN}; run `make -C oracle ref` where the reference tree exists")
+        print(f"missing {REF_BIN}; run `make -C oracle ref REF=<reference tree>` first")
         return 2
     os.makedirs(a.out, exist_ok=True)
     cases = list(CASES) + ([RMAT22] if a.rmat22 else [])

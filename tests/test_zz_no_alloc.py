@@ -84,6 +84,47 @@ def test_noalloc_fp32_weights(lv, graphs):
         assert abs(r[0] - q) <= Q_TOL
 
 
+def test_noalloc_allocates_nothing(lv, golden):
+    """The point of the entry point: once its module is loaded on the device (the first call),
+    a call leaves the device's free memory and torch's reserved pool exactly as they were."""
+    import torch
+    f = _entry(lv)
+    g = golden.load_fixture()
+    row = torch.from_numpy(np.ascontiguousarray(g.row_ptr, dtype=np.int64)).cuda()
+    col = torch.from_numpy(np.ascontiguousarray(g.col, dtype=np.int32)).cuda()
+    lab = torch.arange(g.n, dtype=torch.int32, device="cuda")
+    out = torch.empty(4, dtype=torch.float64, device="cuda")
+    args = (g.n, row.data_ptr(), col.data_ptr(), None, lab.data_ptr(), 1, out.data_ptr(), None)
+    assert f(*args) == 0  # warm call: loads the module and looks up the scratch address
+    torch.cuda.synchronize()
+    free0, reserved0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+    for _ in range(2):
+        assert f(*args) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_reserved() == reserved0
+    r = out.cpu().numpy()
+    assert r[3] == g.m and np.isfinite(r[0])
+
+
+def test_noalloc_flags_bad_input_as_nan(lv, golden):
+    """Checks made on the device: a column outside [0, n) makes Q and m NaN (the call never
+    synchronises, so it cannot return an error for it); a zero total weight gives m = 0 and
+    Q NaN, which out[3] tells apart from bad input."""
+    f = _entry(lv)
+    g = golden.load_fixture()
+    comm = np.arange(g.n, dtype=np.int32)
+    bad = type(g)(n=g.n, row_ptr=g.row_ptr, col=g.col.copy())
+    bad.col[5] = g.n + 3
+    r = _noalloc_q(f, bad, comm, True)
+    assert np.isnan(r[0]) and np.isnan(r[3])
+    zero = type(g)(n=g.n, row_ptr=g.row_ptr, col=g.col, w=np.zeros(len(g.col), dtype=np.float32))
+    r = _noalloc_q(f, zero, comm, False)
+    assert np.isnan(r[0]) and r[3] == 0.0
+    r = _noalloc_q(f, g, comm, True)  # the next call after bad input is clean again
+    assert np.isfinite(r[0]) and r[3] == g.m
+
+
 def test_noalloc_rejects_graph_beyond_scratch(lv):
     f = _entry(lv)
     dummy = ctypes.c_void_p(16)  # never dereferenced: the size check comes first
