@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--mode", default="SORT", choices=["SORT", "HASH"])
     ap.add_argument("--cpu-sample-scale", type=int, default=21)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-summaries", action="store_true",
+                    help="skip the compact batched / served records of the default line")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build beside the default line")
     ap.add_argument("--once", action="store_true",
@@ -296,7 +298,7 @@ def reference_cuda(g, args, runs=2):
     return r
 
 
-def run_batched(args, local):
+def run_batched(args, local, emit=True):
     """4,096 Chung-Lu graphs (exponent 2.1, mean degree 8, n log-uniform in [200, 200,000])
     in one lv_run_batch call, against the same graphs run one lv_run_csr call at a time."""
     import importlib
@@ -374,10 +376,12 @@ def run_batched(args, local):
     }
     line["graph_launches"] = int(st.graph_launches)
     line["autotune"] = tune
-    print(json.dumps(line), flush=True)
     eng.close()
     plain.close()
-    return 0
+    if emit:
+        print(json.dumps(line), flush=True)
+        return 0
+    return line
 
 
 def _percentile(xs, p):
@@ -388,7 +392,7 @@ def _percentile(xs, p):
     return xs[k]
 
 
-def run_served(args, local):
+def run_served(args, local, emit=True):
     """Poisson arrivals of R-MAT requests (edge factor 8, n log-uniform in [1,000, 2,000,000])
     into the server (150 GB budget, `slots` concurrent streams), swept over arrival rates,
     against the same requests run one lv_run_csr call at a time from the same host buffers."""
@@ -489,10 +493,12 @@ def run_served(args, local):
         "clocks": clk.summary(),
         "autotune": tune,
     }
-    print(json.dumps(line), flush=True)
     srv.close()
     eng.close()
-    return 0
+    if emit:
+        print(json.dumps(line), flush=True)
+        return 0
+    return line
 
 
 def run_ingest(args, local):
@@ -546,6 +552,38 @@ def run_ingest(args, local):
     print(json.dumps(line), flush=True)
     eng.close()
     return 0
+
+
+def system_summaries(args, local):
+    """Compact records of the two systems workloads beside the default line: the 4,096-graph
+    batch (2 timed steps, built-in bins) against its loop of single calls, and the served
+    stream at its saturated rate (2,000 requests/s, pool of 64) against its loop."""
+    out = {}
+    for name, fn, over in (
+            ("batched", run_batched, {"steps": 2, "warmup": 1, "graphs": 4096, "no_autotune": True}),
+            ("served", run_served, {"rates": "2000", "pool": 64, "slots": 16, "no_autotune": True,
+                                    "captured": -1})):
+        a = argparse.Namespace(**vars(args))
+        for k, v in over.items():
+            setattr(a, k, v)
+        try:
+            r = fn(a, local, emit=False)
+        except Exception as e:  # the headline line must still print
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            continue
+        if name == "batched":
+            out[name] = {"graphs_per_s": r["value"], "ms_per_batch": r["ms_per_step"],
+                         "loop_graphs_per_s": r["loop"]["graphs_per_s"],
+                         "speedup_vs_loop": r["speedup_vs_loop"], "parity": r["parity"],
+                         "config": r["config"], "steps": a.steps, "warmup": a.warmup}
+        else:
+            rr = r["rates"][0]
+            out[name] = {"graphs_per_s": rr["graphs_per_s"], "p50_ms": rr["p50_ms"],
+                         "p99_ms": rr["p99_ms"], "rate": rr["rate"], "requests": rr["requests"],
+                         "loop_graphs_per_s": r["loop"]["graphs_per_s"],
+                         "speedup_vs_loop": r["speedup_vs_loop"], "parity": r["parity"],
+                         "config": r["config"]}
+    return out
 
 
 def run_planted(args, local):
@@ -758,6 +796,9 @@ def main():
             rc["speedup_e2e_vs_call"] = rc["call_ms"] / (e2e_sec * 1e3)
             rc["same_modularity"] = abs(rc["modularity"] - q) <= 1e-6
         line["reference_cuda"] = rc
+    if rank == 0 and world == 1 and not args.no_summaries:
+        eng.close()
+        line.update(system_summaries(args, local))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args)
     if rank == 0:

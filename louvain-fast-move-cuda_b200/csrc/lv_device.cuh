@@ -173,6 +173,25 @@ __device__ __forceinline__ float gain_upper(float diff, double p, double inv_m, 
   return __double2float_ru(__dadd_ru(__dadd_rn(t1, t2), err));
 }
 
+// The reference's gain (gain_exact's float result, bit for bit) without dividing, in almost
+// every case. With s = rn(t1 + t2) and err as in gain_upper, the reference's double sum X lies
+// in [rd(s - err), ru(s + err)]; rounding to float is monotone, so when both ends of that
+// interval round to the same float (compared bit for bit, so that -0 and +0 differ), that float
+// is rn_f32(X) -- the test of Ziv's strategy for correctly rounded evaluation. Only when X may
+// sit at a float rounding boundary (a relative window of about 2^-45 around one of them, so
+// almost never) is the division-based gain_exact evaluated.
+__device__ __forceinline__ float gain_fast(float diff, double p, double inv_m, double inv_2m2,
+                                           double m, double two_m2) {
+  const double t1 = __dmul_rn((double)diff, inv_m);
+  const double t2 = __dmul_rn(p, inv_2m2);
+  const double err = __fma_rn(__dadd_rn(fabs(t1), fabs(t2)), 0x1p-49, 0x1p-1000);
+  const double s = __dadd_rn(t1, t2);
+  const float lo = __double2float_rn(__dsub_rd(s, err));
+  const float hi = __double2float_rn(__dadd_ru(s, err));
+  if (__float_as_uint(lo) == __float_as_uint(hi)) return lo;
+  return gain_exact(diff, p, m, two_m2);
+}
+
 // Argmax key for a positive gain: the float bits order positive floats, the low word breaks
 // ties -- ~c makes the lowest community win (SORT: GetMaxValue keeps the first of equal
 // values in ascending community order, operators.h:30-40), c makes the highest win (HASH:

@@ -339,7 +339,7 @@ class Run {
     const size_t slot = opt_slot_bytes();  // the gain kernels' tables are the larger ones
     int max_smem = 0;
     LV_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    if ((size_t)block_cap * slot > (size_t)max_smem - 1024)
+    if ((size_t)block_cap * slot > (size_t)max_smem - 1024 || block_cap > 65536)
       throw Fail{LV_ERR_ARGUMENT, "bin 6 table does not fit shared memory"};
     for (int b = 0; b < 6; ++b)
       if ((size_t)(256 / kTeamT[b]) * team_cap[b] * slot > (size_t)max_smem - 1024)
@@ -347,9 +347,9 @@ class Run {
   }
 
   // Shared memory per table slot: the contraction's tables (key + sum) and the gain kernels'
-  // (key + sum, plus half a u32 of key list per slot: the list holds cap / 2 slot indices).
+  // (key + sum, plus half a u16 of key list per slot: the list holds cap / 2 slot indices).
   size_t con_slot_bytes() const { return 4 + acc_size(); }
-  size_t opt_slot_bytes() const { return 4 + acc_size() + 2; }
+  size_t opt_slot_bytes() const { return 4 + acc_size() + 1; }
 
   template <int T>
   void team_grid(int b, const void* opt_fn, const void* con_fn) {
@@ -734,8 +734,17 @@ class Run {
     LV_CUDA(cudaEventElapsedTime(&mk, ev[4], ev[5]));
     t_opt_ms += ms;
     t_optk_ms += mk;
+    if (debug) {
+      const auto ve = read_ctrl<unsigned long long>(offsetof(Ctrl, act_vertices_total));
+      const auto ee = read_ctrl<unsigned long long>(offsetof(Ctrl, act_entries_total));
+      std::fprintf(stderr, "[lv] pass level=%d n=%u E=%u active_v=%llu active_e=%llu ms=%.3f opt_ms=%.3f\n",
+                   levels_run, n, E, ve - dbg_v, ee - dbg_e, ms, mk);
+      dbg_v = ve;
+      dbg_e = ee;
+    }
     return left;
   }
+  unsigned long long dbg_v = 0, dbg_e = 0;  // LV_DEBUG: totals at the previous pass
 
   void force_iterating() {
     // phase-level API: an explicit pass on a graph whose level loop already stopped

@@ -11,13 +11,18 @@
 //   tokens   : per-thread byte chunks count token starts, a scan places them, one thread per
 //              token parses it (optional sign and decimal digits, int32 range); the input ends
 //              at the first token that is not an integer, and an unpaired last token is dropped
-//   ids      : min / max reduction, a presence bitmap over [min, max] (ids must fill it)
-//   pairs    : (min, max) keys radix-sorted and deduplicated (n_links)
-//   CSR      : both directions of every pair (a self-loop pair gives two (u, u) entries),
-//              radix-sorted by (source, destination), row offsets from the sorted sources
+//   ids      : min / max reduction; every pair counts one entry into the row of each end,
+//              and every id in [min, max] must have a row (ids must be contiguous)
+//   rows     : a scan of the counts places the rows; every pair writes each end into the
+//              other's row (a self-loop pair writes its id twice into its own row)
+//   CSR      : each row sorted and deduplicated on its own -- a warp bitonic sort in registers
+//              for rows of up to 32 entries, a block bitonic sort in shared memory up to
+//              kIngestBlockRow, and above that a bitmap of the row's id range in global memory
+//              whose set bits read out in order are the sorted distinct ids; a row keeps its
+//              own id twice when the graph has that self-loop pair (graph.cu:68-79 emits both
+//              directions of it); a second scan of the row lengths gives the row offsets
+// Every scan is the file's own (k_iscan_*), so no library sort or scan is on this path.
 #pragma once
-
-#include <cub/cub.cuh>
 
 namespace lv {
 
@@ -101,49 +106,285 @@ __global__ void k_ids_minmax(const int32_t* val, uint64_t nt, int* mn, int* mx) 
   }
 }
 
-// Presence of every id, and the pair keys (min id << 32 | max id), ids relative to the minimum.
-__global__ void k_ids_mark(const int32_t* val, uint64_t npairs, int mn, uint8_t* present, uint64_t* keys) {
-  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
-       p += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t a = (uint32_t)((long long)val[2 * p] - mn), b = (uint32_t)((long long)val[2 * p + 1] - mn);
-    present[a] = 1;
-    present[b] = 1;
-    keys[p] = a < b ? ((uint64_t)a << 32) | b : ((uint64_t)b << 32) | a;
+// ---- device-wide exclusive scan (u32 in, T out) over tiles of kIScanTile elements ------------
+constexpr int kIScanNT = 256;
+constexpr int kIScanPer = 8;
+constexpr uint32_t kIScanTile = kIScanNT * kIScanPer;
+
+template <class T>
+__global__ void __launch_bounds__(kIScanNT) k_iscan_tiles(const uint32_t* in, uint64_t n, T* tile_sums) {
+  __shared__ T sh[33];
+  const uint64_t ntiles = (n + kIScanTile - 1) / kIScanTile;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t b = t * kIScanTile + (uint64_t)threadIdx.x * kIScanPer;
+    T x = 0;
+#pragma unroll
+    for (int i = 0; i < kIScanPer; ++i)
+      if (b + i < n) x += (T)in[b + i];
+    T tot;
+    block_excl_scan<T, kIScanNT>(x, sh, &tot);
+    if (threadIdx.x == 0) tile_sums[t] = tot;
   }
 }
 
-__global__ void k_count_present(const uint8_t* present, uint64_t range, unsigned long long* count) {
+// One block: tile sums -> exclusive tile offsets (in place); *total = the sum of everything.
+template <class T>
+__global__ void __launch_bounds__(1024) k_iscan_sums(T* tile_sums, uint64_t ntiles, T* total) {
+  __shared__ T sh[33];
+  const uint64_t per = (ntiles + 1023) / 1024;
+  const uint64_t b = (uint64_t)threadIdx.x * per, e = min(ntiles, b + per);
+  T x = 0;
+  for (uint64_t i = b; i < e; ++i) x += tile_sums[i];
+  T tot;
+  T run = block_excl_scan<T, 1024>(x, sh, &tot);
+  for (uint64_t i = b; i < e; ++i) {
+    const T y = tile_sums[i];
+    tile_sums[i] = run;
+    run += y;
+  }
+  if (threadIdx.x == 0) *total = tot;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kIScanNT) k_iscan_apply(const uint32_t* in, uint64_t n, const T* tile_offs,
+                                                          T* out) {
+  __shared__ T sh[33];
+  const uint64_t ntiles = (n + kIScanTile - 1) / kIScanTile;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t b = t * kIScanTile + (uint64_t)threadIdx.x * kIScanPer;
+    T v[kIScanPer];
+    T x = 0;
+#pragma unroll
+    for (int i = 0; i < kIScanPer; ++i) {
+      v[i] = b + i < n ? (T)in[b + i] : T(0);
+      x += v[i];
+    }
+    T run = block_excl_scan<T, kIScanNT>(x, sh, nullptr) + tile_offs[t];
+#pragma unroll
+    for (int i = 0; i < kIScanPer; ++i)
+      if (b + i < n) {
+        out[b + i] = run;
+        run += v[i];
+      }
+  }
+}
+
+// ---- rows ----------------------------------------------------------------------------------
+// Entries per row: each pair puts one entry into the row of each end (ids relative to the
+// minimum); a row with no entry means a missing id.
+__global__ void k_pair_count(const int32_t* val, uint64_t npairs, int mn, uint32_t* cnt) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
+       p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = (uint32_t)((long long)val[2 * p] - mn), b = (uint32_t)((long long)val[2 * p + 1] - mn);
+    atomicAdd(&cnt[a], 1u);
+    atomicAdd(&cnt[b], 1u);
+  }
+}
+
+__global__ void k_count_present(const uint32_t* cnt, uint64_t range, unsigned long long* count) {
   unsigned long long c = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < range; i += (uint64_t)gridDim.x * blockDim.x)
-    c += present[i];
+    c += cnt[i] != 0u;
   c = warp_sum(c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
-// Distinct sorted pair keys -> both directions as (source << 32 | destination).
-__global__ void k_pairs_both(const uint64_t* uniq, uint64_t nl, uint64_t* both) {
-  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < nl; p += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = uniq[p];
-    both[2 * p] = k;
-    both[2 * p + 1] = (k << 32) | (k >> 32);
+// Every pair writes each end into the other end's row (cursor starts at the row starts).
+__global__ void k_pair_scatter(const int32_t* val, uint64_t npairs, int mn, uint32_t* cursor, uint32_t* buf) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
+       p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = (uint32_t)((long long)val[2 * p] - mn), b = (uint32_t)((long long)val[2 * p + 1] - mn);
+    buf[atomicAdd(&cursor[a], 1u)] = b;
+    buf[atomicAdd(&cursor[b], 1u)] = a;
   }
 }
 
-// Sorted (source, destination) keys -> col, and each row's first entry index.
-__global__ void k_csr_fill(const uint64_t* sorted, uint64_t ne, int32_t* col, unsigned long long* rowstart) {
-  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = sorted[e];
-    col[e] = (int32_t)(uint32_t)k;
-    const uint32_t s = (uint32_t)(k >> 32);
-    if (e == 0 || (uint32_t)(sorted[e - 1] >> 32) != s) rowstart[s] = e;
+constexpr uint32_t kIngestWarpRow = 32;     // rows sorted by one warp in registers
+constexpr uint32_t kIngestBlockRow = 4096;  // rows sorted by one block in shared memory
+constexpr int kIngestBlockNT = 512;
+
+// Rows longer than a warp's: appended to the block list or the bitmap list.
+__global__ void k_rows_classify(const uint32_t* cnt, uint32_t range, uint32_t* mid, uint32_t* big,
+                                uint32_t* counts) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < range; base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + threadIdx.x;
+    const uint32_t c = v < range ? cnt[v] : 0u;
+    const int cls = c > kIngestBlockRow ? 1 : (c > kIngestWarpRow ? 0 : -1);
+    const uint32_t pm = warp_append(cls, 0, &counts[0]);
+    if (pm != kEmpty) mid[pm] = v;
+    const uint32_t pb = warp_append(cls, 1, &counts[1]);
+    if (pb != kEmpty) big[pb] = v;
   }
 }
 
-// Row starts recorded at each row's first entry; every vertex has at least one entry (the ids
-// are contiguous and each appears in a pair), so every row was written.
-__global__ void k_csr_rows(const unsigned long long* rowstart, uint32_t n, uint64_t ne, int64_t* row_ptr) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
-    row_ptr[v] = v == n ? (int64_t)ne : (int64_t)rowstart[v];
+// Rows of up to 32 entries, one warp each: bitonic sort across the lanes, then the distinct
+// ids written back to the row's start in order (the row's own id twice), length to ulen.
+__global__ void k_rows_warp(const uint32_t* start, const uint32_t* cnt, uint32_t range, uint32_t* buf,
+                            uint32_t* ulen) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = warp; v < range; v += nwarps) {
+    const uint32_t c = cnt[v];
+    if (c > kIngestWarpRow) continue;  // (warp-uniform)
+    const uint32_t s0 = start[v];
+    uint32_t x = (uint32_t)lane < c ? buf[s0 + lane] : kEmpty;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const uint32_t y = __shfl_xor_sync(kFull, x, j);
+        const bool up = (lane & k) == 0, low = (lane & j) == 0;
+        x = (low == up) ? min(x, y) : max(x, y);
+      }
+    }
+    const uint32_t prev = __shfl_up_sync(kFull, x, 1);
+    const bool keep = x != kEmpty && (lane == 0 || x != prev);
+    const uint32_t emit = keep ? (x == v ? 2u : 1u) : 0u;
+    const uint32_t incl = warp_incl_scan(emit, lane);
+    const uint32_t tot = __shfl_sync(kFull, incl, 31);
+    __syncwarp();
+    for (uint32_t i = 0; i < emit; ++i) buf[s0 + incl - emit + i] = x;
+    if (lane == 0) ulen[v] = tot;
+  }
+}
+
+// Rows of 33..kIngestBlockRow entries, one block each: bitonic sort in shared memory.
+__global__ void __launch_bounds__(kIngestBlockNT) k_rows_block(const uint32_t* start, const uint32_t* cnt,
+                                                               const uint32_t* mid, const uint32_t* counts,
+                                                               uint32_t* buf, uint32_t* ulen) {
+  __shared__ uint32_t sv[kIngestBlockRow];
+  __shared__ uint32_t sh[33];
+  constexpr uint32_t PER = kIngestBlockRow / kIngestBlockNT;
+  const uint32_t nmid = counts[0];
+  for (uint32_t r = blockIdx.x; r < nmid; r += gridDim.x) {
+    const uint32_t v = mid[r];
+    const uint32_t c = cnt[v], s0 = start[v];
+    uint32_t P = 64;
+    while (P < c) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += kIngestBlockNT) sv[i] = i < c ? buf[s0 + i] : kEmpty;
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < P; i += kIngestBlockNT) {
+          const uint32_t ixj = i ^ j;
+          if (ixj > i) {
+            const uint32_t a = sv[i], b = sv[ixj];
+            const bool up = (i & k) == 0;
+            if ((a > b) == up) {
+              sv[i] = b;
+              sv[ixj] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // thread t owns elements [t*PER, t*PER + PER) of the sorted row
+    uint32_t emit = 0;
+    const uint32_t b0 = threadIdx.x * PER;
+#pragma unroll
+    for (uint32_t i = 0; i < PER; ++i) {
+      const uint32_t q = b0 + i;
+      if (q < P) {
+        const uint32_t x = sv[q];
+        if (x != kEmpty && (q == 0 || sv[q - 1] != x)) emit += x == v ? 2u : 1u;
+      }
+    }
+    uint32_t tot;
+    uint32_t off = block_excl_scan<uint32_t, kIngestBlockNT>(emit, sh, &tot);
+#pragma unroll
+    for (uint32_t i = 0; i < PER; ++i) {
+      const uint32_t q = b0 + i;
+      if (q < P) {
+        const uint32_t x = sv[q];
+        if (x != kEmpty && (q == 0 || sv[q - 1] != x)) {
+          buf[s0 + off++] = x;
+          if (x == v) buf[s0 + off++] = x;
+        }
+      }
+    }
+    if (threadIdx.x == 0) ulen[v] = tot;
+    __syncthreads();
+  }
+}
+
+// Rows above kIngestBlockRow entries, one block each with its own bitmap (bmw words) of the
+// row's id range [lo, hi]: set bits, then read them out in order.
+__global__ void __launch_bounds__(kIngestBlockNT) k_rows_bitmap(const uint32_t* start, const uint32_t* cnt,
+                                                                const uint32_t* big, const uint32_t* counts,
+                                                                uint32_t* bitmaps, uint64_t bmw,
+                                                                uint32_t* buf, uint32_t* ulen) {
+  __shared__ uint32_t sh[33];
+  __shared__ uint32_t lo_sh, hi_sh;
+  uint32_t* bm = bitmaps + (uint64_t)blockIdx.x * bmw;
+  const uint32_t nbig = counts[1];
+  for (uint32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const uint32_t v = big[r];
+    const uint32_t c = cnt[v], s0 = start[v];
+    uint32_t lo = kEmpty, hi = 0;
+    for (uint32_t i = threadIdx.x; i < c; i += kIngestBlockNT) {
+      const uint32_t x = buf[s0 + i];
+      lo = min(lo, x);
+      hi = max(hi, x);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+      hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    if (threadIdx.x == 0) { lo_sh = kEmpty; hi_sh = 0; }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) { atomicMin(&lo_sh, lo); atomicMax(&hi_sh, hi); }
+    __syncthreads();
+    lo = lo_sh;
+    hi = hi_sh;
+    const uint32_t words = ((hi - lo) >> 5) + 1;  // <= bmw
+    for (uint32_t i = threadIdx.x; i < words; i += kIngestBlockNT) bm[i] = 0u;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < c; i += kIngestBlockNT) {
+      const uint32_t d = buf[s0 + i] - lo;
+      atomicOr(&bm[d >> 5], 1u << (d & 31));
+    }
+    __syncthreads();
+    // thread t reads a contiguous run of words; counts, block scan, then the ids in order
+    const uint32_t per = (words + kIngestBlockNT - 1) / kIngestBlockNT;
+    const uint32_t w0 = threadIdx.x * per, w1 = min(words, w0 + per);
+    const uint32_t self_w = v >= lo && v <= hi ? (v - lo) >> 5 : kEmpty;
+    uint32_t emit = 0;
+    for (uint32_t i = w0; i < w1; ++i) {
+      const uint32_t m = bm[i];
+      emit += __popc(m);
+      if (i == self_w && ((m >> ((v - lo) & 31)) & 1u)) emit += 1;  // the self-loop twice
+    }
+    uint32_t tot;
+    uint32_t off = block_excl_scan<uint32_t, kIngestBlockNT>(emit, sh, &tot);
+    __syncthreads();  // every id was read into the bitmap before any is overwritten
+    for (uint32_t i = w0; i < w1; ++i) {
+      uint32_t m = bm[i];
+      while (m) {
+        const uint32_t bit = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t x = lo + (i << 5) + bit;
+        buf[s0 + off++] = x;
+        if (x == v) buf[s0 + off++] = x;
+      }
+    }
+    if (threadIdx.x == 0) ulen[v] = tot;
+    __syncthreads();
+  }
+}
+
+// Distinct, sorted rows (at their bucket starts) -> the dense CSR, a warp per row.
+__global__ void k_rows_copy(const uint32_t* start, const uint32_t* ulen, const int64_t* row_ptr, uint32_t range,
+                            const uint32_t* buf, int32_t* col) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = warp; v < range; v += nwarps) {
+    const uint32_t s0 = start[v], len = ulen[v];
+    const int64_t d0 = row_ptr[v];
+    for (uint32_t i = lane; i < len; i += 32) col[d0 + i] = (int32_t)buf[s0 + i];
+  }
 }
 
 }  // namespace lv
@@ -176,6 +417,18 @@ struct DevBuf {
     return reinterpret_cast<T*>(p);
   }
 };
+
+// Exclusive scan of n u32 counts into out (T = u32 or i64): tile sums, one block over them,
+// then each tile again with its offset. `tmp` holds the tile sums.
+template <class T>
+static void iscan(lv_context* ctx, cudaStream_t st, DevBuf& tmp, const uint32_t* in, uint64_t n, T* out) {
+  const uint64_t ntiles = (n + kIScanTile - 1) / kIScanTile;
+  T* sums = tmp.alloc<T>(ntiles + 1);
+  const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * 8);
+  k_iscan_tiles<T><<<grid, kIScanNT, 0, st>>>(in, n, sums);
+  k_iscan_sums<T><<<1, 1024, 0, st>>>(sums, ntiles, sums + ntiles);
+  k_iscan_apply<T><<<grid, kIScanNT, 0, st>>>(in, n, sums, out);
+}
 
 static void ingest_run(lv_context* ctx, const char* text_in, int64_t len, int32_t skip_line, int32_t in_mem,
                        lv_ingest* out) {
@@ -226,10 +479,7 @@ static void ingest_run(lv_context* ctx, const char* text_in, int64_t len, int32_
   uint32_t* off = boff.alloc<uint32_t>(nchunks + 1);
   k_tok_count<<<grid, 256, 0, st>>>(text, L, cnt, nchunks);
   LV_CUDA(cudaMemsetAsync(cnt + nchunks, 0, 4, st));
-  size_t tb = 0;
-  LV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)(nchunks + 1), st));
-  void* tmp = btmp.alloc<unsigned char>(tb);
-  LV_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, (int)(nchunks + 1), st));
+  iscan<uint32_t>(ctx, st, btmp, cnt, nchunks + 1, off);
   uint32_t ntok32 = 0;
   LV_CUDA(cudaMemcpyAsync(&ntok32, off + nchunks, 4, cudaMemcpyDeviceToHost, st));
   LV_CUDA(cudaStreamSynchronize(st));
@@ -264,64 +514,71 @@ static void ingest_run(lv_context* ctx, const char* text_in, int64_t len, int32_
   const uint64_t range = (uint64_t)((long long)hmm[1] - (long long)hmm[0] + 1);
   // contiguous ids: at most one id per token, so a wider range cannot be filled
   if (range > 2 * npairs) throw Fail{LV_ERR_INPUT, "vertex IDs must be contiguous (the reference indexes by id - min_id)"};
-  DevBuf bpres, bkeys, bcount;
-  uint8_t* present = bpres.alloc<uint8_t>(range);
-  LV_CUDA(cudaMemsetAsync(present, 0, range, st));
-  uint64_t* keys = bkeys.alloc<uint64_t>(npairs);
-  k_ids_mark<<<grid, 256, 0, st>>>(val, npairs, hmm[0], present, keys);
-  unsigned long long* pc = bcount.alloc<unsigned long long>(1);
-  LV_CUDA(cudaMemsetAsync(pc, 0, 8, st));
-  k_count_present<<<grid, 256, 0, st>>>(present, range, pc);
+  if (range >= 0x7FFFFFFFull) throw Fail{LV_ERR_RANGE, "more than 2^31-1 vertices"};
+  // entries per row (both ends of every pair); every id must have one
+  DevBuf bcntr, bstart, bcount;
+  uint32_t* cntr = bcntr.alloc<uint32_t>(range + 1);
+  LV_CUDA(cudaMemsetAsync(cntr, 0, (range + 1) * 4, st));
+  k_pair_count<<<grid, 256, 0, st>>>(val, npairs, hmm[0], cntr);
+  unsigned long long* pc = bcount.alloc<unsigned long long>(2);
+  LV_CUDA(cudaMemsetAsync(pc, 0, 16, st));
+  k_count_present<<<grid, 256, 0, st>>>(cntr, range, pc);
   unsigned long long nn = 0;
   LV_CUDA(cudaMemcpyAsync(&nn, pc, 8, cudaMemcpyDeviceToHost, st));
   LV_CUDA(cudaStreamSynchronize(st));
   if (nn != range) throw Fail{LV_ERR_INPUT, "vertex IDs must be contiguous (the reference indexes by id - min_id)"};
-  if (range >= 0x7FFFFFFFull) throw Fail{LV_ERR_RANGE, "more than 2^31-1 vertices"};
+  // rows placed by a scan of the counts, filled by the pairs
+  uint32_t* rstart = bstart.alloc<uint32_t>(range + 1);
+  iscan<uint32_t>(ctx, st, btmp, cntr, range + 1, rstart);
+  DevBuf bcur, bbuf;
+  uint32_t* cursor = bcur.alloc<uint32_t>(range);
+  LV_CUDA(cudaMemcpyAsync(cursor, rstart, range * 4, cudaMemcpyDeviceToDevice, st));
+  uint32_t* buf = bbuf.alloc<uint32_t>(2 * npairs);
+  k_pair_scatter<<<grid, 256, 0, st>>>(val, npairs, hmm[0], cursor, buf);
   bval.reset();
-  bpres.reset();
-  // distinct pairs
-  int bits = 1;
-  while (bits < 32 && (1ull << bits) < range) ++bits;
-  DevBuf bsorted, bsel;
-  uint64_t* sorted = bsorted.alloc<uint64_t>(npairs);
-  tb = 0;
-  LV_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, sorted, (int)npairs, 0, 32 + bits, st));
-  tmp = btmp.alloc<unsigned char>(tb);
-  LV_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tb, keys, sorted, (int)npairs, 0, 32 + bits, st));
-  int* nsel = bsel.alloc<int>(1);
-  tb = 0;
-  LV_CUDA(cub::DeviceSelect::Unique(nullptr, tb, sorted, keys, nsel, (int)npairs, st));
-  tmp = btmp.alloc<unsigned char>(tb);
-  LV_CUDA(cub::DeviceSelect::Unique(tmp, tb, sorted, keys, nsel, (int)npairs, st));
-  int nl = 0;
-  LV_CUDA(cudaMemcpyAsync(&nl, nsel, 4, cudaMemcpyDeviceToHost, st));
+  // each row sorted and deduplicated in place: warp, block or bitmap by its length
+  DevBuf bmid, bbig, bcls, bulen;
+  uint32_t* mid = bmid.alloc<uint32_t>(range);
+  uint32_t* big = bbig.alloc<uint32_t>(range);
+  uint32_t* cls = bcls.alloc<uint32_t>(2);
+  LV_CUDA(cudaMemsetAsync(cls, 0, 8, st));
+  k_rows_classify<<<grid, 256, 0, st>>>(cntr, (uint32_t)range, mid, big, cls);
+  uint32_t hcls[2] = {0, 0};
+  LV_CUDA(cudaMemcpyAsync(hcls, cls, 8, cudaMemcpyDeviceToHost, st));
+  uint32_t* ulen = bulen.alloc<uint32_t>(range + 1);
+  LV_CUDA(cudaMemsetAsync(ulen + range, 0, 4, st));
+  k_rows_warp<<<grid, 256, 0, st>>>(rstart, cntr, (uint32_t)range, buf, ulen);
+  k_rows_block<<<ctx->sms * 2, kIngestBlockNT, 0, st>>>(rstart, cntr, mid, cls, buf, ulen);
   LV_CUDA(cudaStreamSynchronize(st));
-  const uint64_t ne = 2ull * (uint64_t)nl;
-  // both directions, sorted by (source, destination)
-  DevBuf bboth, bsorted2;
-  uint64_t* both = bboth.alloc<uint64_t>(ne);
-  k_pairs_both<<<grid, 256, 0, st>>>(keys, (uint64_t)nl, both);
-  bkeys.reset();
-  bsorted.reset();
-  uint64_t* sorted2 = bsorted2.alloc<uint64_t>(ne);
-  tb = 0;
-  LV_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, both, sorted2, (int)ne, 0, 32 + bits, st));
-  tmp = btmp.alloc<unsigned char>(tb);
-  LV_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tb, both, sorted2, (int)ne, 0, 32 + bits, st));
-  bboth.reset();
-  // CSR
+  DevBuf bbm;
+  if (hcls[1] > 0) {
+    // a bitmap per block, each as wide as the whole id range; blocks limited to 1 GiB of them
+    const uint64_t bmw = (range >> 5) + 1;
+    const uint64_t nb = std::max<uint64_t>(1, std::min<uint64_t>({(uint64_t)hcls[1], (uint64_t)ctx->sms,
+                                                                   (1ull << 28) / bmw}));
+    uint32_t* bitmaps = bbm.alloc<uint32_t>(nb * bmw);
+    k_rows_bitmap<<<(unsigned)nb, kIngestBlockNT, 0, st>>>(rstart, cntr, big, cls, bitmaps, bmw, buf, ulen);
+  }
+  // the dense CSR: row offsets from a scan of the distinct lengths
   int64_t* row_ptr = nullptr;
   int32_t* col = nullptr;
   LV_CUDA(cudaMalloc(&row_ptr, (range + 1) * sizeof(int64_t)));
-  if (cudaMalloc(&col, ne * sizeof(int32_t)) != cudaSuccess) {
+  iscan<int64_t>(ctx, st, btmp, ulen, range + 1, row_ptr);
+  int64_t ne64 = 0;
+  LV_CUDA(cudaMemcpyAsync(&ne64, row_ptr + range, 8, cudaMemcpyDeviceToHost, st));
+  const cudaError_t e0 = cudaStreamSynchronize(st);
+  if (e0 != cudaSuccess) {
+    cudaFree(row_ptr);
+    throw Fail{LV_ERR_CUDA, std::string("ingest: ") + cudaGetErrorString(e0)};
+  }
+  const uint64_t ne = (uint64_t)ne64;
+  const int64_t nl = ne64 / 2;  // each distinct pair is two entries (a self-loop: its id twice)
+  if (cudaMalloc(&col, std::max<uint64_t>(ne, 1) * sizeof(int32_t)) != cudaSuccess) {
     cudaFree(row_ptr);
     cudaGetLastError();
     throw Fail{LV_ERR_NOMEM, "cudaMalloc of the CSR destinations failed"};
   }
-  DevBuf bstart;
-  unsigned long long* rstart = bstart.alloc<unsigned long long>(range);
-  k_csr_fill<<<grid, 256, 0, st>>>(sorted2, ne, col, rstart);
-  k_csr_rows<<<grid, 256, 0, st>>>(rstart, (uint32_t)range, ne, row_ptr);
+  k_rows_copy<<<grid, 256, 0, st>>>(rstart, ulen, row_ptr, (uint32_t)range, buf, col);
   const cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaFree(row_ptr);

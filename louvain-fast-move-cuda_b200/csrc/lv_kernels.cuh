@@ -289,7 +289,6 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
   using Wt = typename Tr::W;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   unsigned long long best = 0;
-  float bestg = 0.0f;  // gain of `best` (0 while there is none)
   for (uint32_t e = e0; e < x.re; e += kBatch * step) {
     uint32_t uu[kBatch];
     float wf[kBatch];
@@ -308,14 +307,10 @@ __device__ __forceinline__ unsigned long long fast_scan(const Dev& D, const VtxC
       if (uu[k] == v) continue;
       // self = 0: diff = w - 0 = w exactly
       const double p = gain_p(x.kv, x.own_minus_k, au[k]);
-      // the division-free bound discards every entry that cannot reach the best gain so far
-      const float hi = gain_upper(wf[k], p, x.inv_m, x.inv_2m2);
-      if (hi > 0.0f && hi >= bestg) {
-        const float g = gain_exact(wf[k], p, x.m, x.two_m2);
-        if (g > 0.0f) {
-          const unsigned long long key = argmax_key(g, uu[k], true);
-          if (key > best) { best = key; bestg = g; }
-        }
+      const float g = gain_fast(wf[k], p, x.inv_m, x.inv_2m2, x.m, x.two_m2);
+      if (g > 0.0f) {
+        const unsigned long long key = argmax_key(g, uu[k], true);
+        if (key > best) best = key;
       }
     }
   }
@@ -361,7 +356,6 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   unsigned long long best = 0;
-  float bestg = 0.0f;  // gain of `best` (0 while there is none)
   for (uint32_t s = s0; s < cap; s += kBatch * step) {
     uint32_t cc[kBatch];
     Acc vv[kBatch];
@@ -381,13 +375,10 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
       if (cc[k] == kEmpty) continue;
       const float diff = __fsub_rn(Tr::to_float(vv[k]), self_v);
       const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
-      const float hi = gain_upper(diff, p, x.inv_m, x.inv_2m2);
-      if (hi > 0.0f && hi >= bestg) {
-        const float g = gain_exact(diff, p, x.m, x.two_m2);
-        if (g > 0.0f) {
-          const unsigned long long key = argmax_key(g, cc[k], lowest);
-          if (key > best) { best = key; bestg = g; }
-        }
+      const float g = gain_fast(diff, p, x.inv_m, x.inv_2m2, x.m, x.two_m2);
+      if (g > 0.0f) {
+        const unsigned long long key = argmax_key(g, cc[k], lowest);
+        if (key > best) best = key;
       }
     }
   }
@@ -398,7 +389,7 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 // the table, the slot it sits in, so that the evaluation half reads only those slots (the
 // distinct neighbouring communities) instead of scanning the whole table, and empties only
 // them again -- a table is cleared once when a kernel starts and stays empty between vertices.
-// The list has room for min(d, ng) slots, half the table's capacity.
+// The list has room for min(d, ng) slots, half the table's capacity, as u16 indices.
 //
 // Insert half. The entries of the row are walked in team-uniform steps (every lane of the team
 // takes the same number of steps, lanes past the row's end carry nothing), so the lanes that
@@ -409,7 +400,7 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 template <bool WINT, bool BLOCK, class Tbl>
 __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t lane,
                                                 uint32_t step, unsigned tmask, const Tbl& tbl,
-                                                uint32_t* list, uint32_t* bcount,
+                                                uint16_t* list, uint32_t* bcount,
                                                 typename WTraits<WINT>::Acc& self_acc, uint32_t& err) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
@@ -449,10 +440,10 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
           uint32_t base = 0;
           if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(bcount, (uint32_t)__popc(m));
           base = __shfl_sync(kFull, base, leader);
-          if (made) list[base + __popc(m & lt)] = slot;
+          if (made) list[base + __popc(m & lt)] = (uint16_t)slot;
         }
       } else {
-        if (made) list[nl + __popc(m & lt)] = slot;
+        if (made) list[nl + __popc(m & lt)] = (uint16_t)slot;
         nl += __popc(m);
       }
     }
@@ -464,12 +455,11 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
 // distinct neighbouring communities (as cand_scan), emptying each slot after reading it.
 template <bool WINT, class Tbl>
 __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxCtx& x, const Tbl& tbl,
-                                                        const uint32_t* list, uint32_t i0, uint32_t nl,
+                                                        const uint16_t* list, uint32_t i0, uint32_t nl,
                                                         uint32_t step, float self_v, bool lowest) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   unsigned long long best = 0;
-  float bestg = 0.0f;
   for (uint32_t i = i0; i < nl; i += kBatch * step) {
     uint32_t cc[kBatch];
     Acc vv[kBatch];
@@ -493,13 +483,10 @@ __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxC
       if (cc[k] == kEmpty) continue;
       const float diff = __fsub_rn(Tr::to_float(vv[k]), self_v);
       const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
-      const float hi = gain_upper(diff, p, x.inv_m, x.inv_2m2);
-      if (hi > 0.0f && hi >= bestg) {
-        const float g = gain_exact(diff, p, x.m, x.two_m2);
-        if (g > 0.0f) {
-          const unsigned long long key = argmax_key(g, cc[k], lowest);
-          if (key > best) { best = key; bestg = g; }
-        }
+      const float g = gain_fast(diff, p, x.inv_m, x.inv_2m2, x.m, x.two_m2);
+      if (g > 0.0f) {
+        const unsigned long long key = argmax_key(g, cc[k], lowest);
+        if (key > best) best = key;
       }
     }
   }
@@ -524,12 +511,13 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
   constexpr int TEAMS = 256 / T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int team = threadIdx.x / T, lane = threadIdx.x % T;
-  // per team: a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 slots
+  // per team: a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 u16
+  // slot indices (table capacities stay below 2^16: they must fit shared memory)
   constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
   unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
-  uint32_t* list = reinterpret_cast<uint32_t*>(smem + (size_t)TEAMS * cap * kSlotBytes) + (size_t)team * (cap / 2);
+  uint16_t* list = reinterpret_cast<uint16_t*>(smem + (size_t)TEAMS * cap * kSlotBytes) + (size_t)team * (cap / 2);
 
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
@@ -631,12 +619,12 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long red[33];
   __shared__ uint32_t nlist;
-  // a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 slots
+  // a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 u16 slot indices
   constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
   unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
-  uint32_t* list = reinterpret_cast<uint32_t*>(smem + (size_t)cap * kSlotBytes);
+  uint16_t* list = reinterpret_cast<uint16_t*>(smem + (size_t)cap * kSlotBytes);
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
   if (blockIdx.x >= count) return;  // (block-uniform)
