@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--mode", default="SORT", choices=["SORT", "HASH"])
     ap.add_argument("--cpu-sample-scale", type=int, default=21)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-loop", action="store_true",
+                    help="served: also time the reference's CUDA build once per pool graph")
     ap.add_argument("--no-summaries", action="store_true",
                     help="skip the compact batched / served records of the default line")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -298,6 +300,43 @@ def reference_cuda(g, args, runs=2):
     return r
 
 
+def reference_loop(graphs_list, args):
+    """The reference's own CUDA build run once per graph, as its main.cu loops over datasets
+    (main.cu:19-39): the summed call times around ModularityAlgorithms::Louvain (its Community
+    upload and device graph build included, process start-up and file reading excluded).
+    A graph goes to the reference only if the oracle predicts no overrun of the reference's
+    modularity scratch (community.h:69, an out-of-bounds device write otherwise)."""
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not os.path.exists(REF_CUDA_BIN):
+        return {"unavailable": "oracle/_ref/ref_louvain not built"}
+    call_ms, ran, skipped = 0.0, 0, 0
+    with tempfile.TemporaryDirectory() as d:
+        inp, out = os.path.join(d, "graph.csr"), os.path.join(d, "res.bin")
+        for g in graphs_list:
+            o = O.Oracle(g, mode=O.SORT if args.mode == "SORT" else O.HASH, nthreads=0)
+            o.louvain()
+            if o.overrun_events:
+                skipped += 1
+                continue
+            with open(inp, "wb") as f:
+                np.array([g.n, g.E], dtype=np.int64).tofile(f)
+                np.ascontiguousarray(g.row_ptr, dtype=np.int64).tofile(f)
+                np.ascontiguousarray(g.col, dtype=np.int32).tofile(f)
+            p = subprocess.run([REF_CUDA_BIN, inp, args.mode, out, "csr"], capture_output=True,
+                               text=True, timeout=600)
+            if p.returncode != 0:
+                return {"unavailable": f"reference exited {p.returncode}: {p.stderr[-300:]}"}
+            with open(out, "rb") as f:
+                f.read(16)
+                call_ms += float(np.frombuffer(f.read(4), dtype=np.float32)[0])
+            ran += 1
+    return {"graphs": ran, "skipped_overrun": skipped, "call_ms_sum": call_ms,
+            "graphs_per_s": ran / (call_ms / 1e3) if call_ms > 0 else None,
+            "what": "oracle/_ref/ref_louvain once per graph, summed call times"}
+
+
 def run_batched(args, local, emit=True):
     """4,096 Chung-Lu graphs (exponent 2.1, mean degree 8, n log-uniform in [200, 200,000])
     in one lv_run_batch call, against the same graphs run one lv_run_csr call at a time."""
@@ -434,6 +473,8 @@ def run_served(args, local, emit=True):
     loop_s = time.perf_counter() - t0
     loop_gps = len(pool) / loop_s
 
+    ref_loop = reference_loop(pool, args) if args.reference_loop else None
+
     srv = lv.Server(eng, 150 << 30, slots=args.slots)
     # warm-up: the whole pool twice in a burst, so that every slot captures its level loop and
     # the memory pool holds every size before the timed rates
@@ -490,6 +531,7 @@ def run_served(args, local, emit=True):
                                                     "request from the same pinned host buffers"},
         "speedup_vs_loop": best["graphs_per_s"] / loop_gps,
         "parity": {"max_abs_dq_vs_alone": worst_dq},
+        "reference_loop": ref_loop,
         "clocks": clk.summary(),
         "autotune": tune,
     }

@@ -157,29 +157,17 @@ __device__ __forceinline__ float gain_ref(float w_vc, float self_v, double k, do
   return gain_exact(__fsub_rn(w_vc, self_v), gain_p(k, __dsub_rn(a_own, k), a_c), m, two_m2);
 }
 
-// An upper bound of gain_exact(diff, p, m, two_m2) without division, for discarding candidates
-// that cannot beat the best gain found so far. With r1 = rn(1/m) and r2 = rn(1/two_m2),
-// t1 = rn(diff*r1) and t2 = rn(p*r2) are each within 3 units of 2^-53 (relative) of the exact
-// quotients rn(diff/m) and rn(p/two_m2) (one rounding in the reciprocal, one in the product,
-// one in the quotient), so rn(t1 + t2) is within 5 * 2^-53 * (|t1| + |t2|) of the reference's
-// double sum. err = 2^-49 * (|t1| + |t2|) + 2^-1000 covers that with room to spare (the
-// absolute term covers subnormal results); adding it rounding up and converting to float
-// rounding up gives a float >= the reference's rn-to-float gain, since both roundings are
-// monotone.
-__device__ __forceinline__ float gain_upper(float diff, double p, double inv_m, double inv_2m2) {
-  const double t1 = __dmul_rn((double)diff, inv_m);
-  const double t2 = __dmul_rn(p, inv_2m2);
-  const double err = __fma_rn(__dadd_rn(fabs(t1), fabs(t2)), 0x1p-49, 0x1p-1000);
-  return __double2float_ru(__dadd_ru(__dadd_rn(t1, t2), err));
-}
-
 // The reference's gain (gain_exact's float result, bit for bit) without dividing, in almost
-// every case. With s = rn(t1 + t2) and err as in gain_upper, the reference's double sum X lies
-// in [rd(s - err), ru(s + err)]; rounding to float is monotone, so when both ends of that
-// interval round to the same float (compared bit for bit, so that -0 and +0 differ), that float
-// is rn_f32(X) -- the test of Ziv's strategy for correctly rounded evaluation. Only when X may
-// sit at a float rounding boundary (a relative window of about 2^-45 around one of them, so
-// almost never) is the division-based gain_exact evaluated.
+// every case. With r1 = rn(1/m) and r2 = rn(1/two_m2) (precomputed per graph), t1 = rn(diff*r1)
+// and t2 = rn(p*r2) are each within 3 units of 2^-53 (relative) of the exact quotients
+// rn(diff/m) and rn(p/two_m2) (one rounding in the reciprocal, one in the product, one in the
+// quotient), so s = rn(t1 + t2) is within 5 * 2^-53 * (|t1| + |t2|) of the reference's double
+// sum X. err = 2^-49 * (|t1| + |t2|) + 2^-1000 covers that with room to spare (the absolute
+// term covers subnormal results), so X lies in [rd(s - err), ru(s + err)]. Rounding to float is
+// monotone: when both ends of that interval round to the same float (compared bit for bit, so
+// that -0 and +0 differ), that float is rn_f32(X) -- the test of Ziv's strategy for correctly
+// rounded evaluation. Only when X may sit at a float rounding boundary (a relative window of
+// about 2^-45 around one of them, so almost never) is the division-based gain_exact evaluated.
 __device__ __forceinline__ float gain_fast(float diff, double p, double inv_m, double inv_2m2,
                                            double m, double two_m2) {
   const double t1 = __dmul_rn((double)diff, inv_m);
@@ -323,7 +311,10 @@ struct PackedTable {
   unsigned long long* slots;
   uint32_t mask, shift;
   __device__ __forceinline__ bool add(uint32_t c, uint32_t w) const {
-    uint32_t h = hash_slot(c, shift);
+    return add_from(hash_slot(c, shift), c, w);
+  }
+  // add() with the probe sequence starting at slot h (the home slot, or one past it)
+  __device__ __forceinline__ bool add_from(uint32_t h, uint32_t c, uint32_t w) const {
     for (uint32_t probe = 0; probe <= mask; ++probe) {
       unsigned long long cur = ((volatile unsigned long long*)slots)[h];
       uint32_t key = (uint32_t)(cur >> 32);

@@ -397,7 +397,7 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 // the team's lanes within the warp. BLOCK: the team is the whole block; warps take list space
 // from the shared counter *bcount (one atomic per warp and batch), which the caller reads after
 // a barrier. Otherwise the team is part of one warp and the count is returned.
-template <bool WINT, bool BLOCK, class Tbl>
+template <bool WINT, bool BLOCK, int NB, class Tbl>
 __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t lane,
                                                 uint32_t step, unsigned tmask, const Tbl& tbl,
                                                 uint16_t* list, uint32_t* bcount,
@@ -408,20 +408,20 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   const uint32_t lt = lanemask_lt();
   uint32_t nl = 0;
-  for (uint32_t b = x.rs; b < x.re; b += kBatch * step) {
-    uint32_t uu[kBatch], cc[kBatch];
-    Acc ww[kBatch];
+  for (uint32_t b = x.rs; b < x.re; b += NB * step) {
+    uint32_t uu[NB], cc[NB];
+    Acc ww[NB];
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
+    for (int k = 0; k < NB; ++k) {
       const uint32_t ek = b + lane + k * step;
       const bool in = ek < x.re;
       uu[k] = in ? D.col[ek] : v;
       ww[k] = in ? (x.unit ? Acc(1) : (Acc)w[ek]) : Acc(0);
     }
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+    for (int k = 0; k < NB; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
+    for (int k = 0; k < NB; ++k) {
       bool made = false;
       uint32_t slot = 0;
       if (cc[k] != kEmpty) {
@@ -453,19 +453,19 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
 
 // Evaluation half over the listed slots [i0, nl) with stride `step`: best key over the
 // distinct neighbouring communities (as cand_scan), emptying each slot after reading it.
-template <bool WINT, class Tbl>
+template <bool WINT, int NB, class Tbl>
 __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxCtx& x, const Tbl& tbl,
                                                         const uint16_t* list, uint32_t i0, uint32_t nl,
                                                         uint32_t step, float self_v, bool lowest) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   unsigned long long best = 0;
-  for (uint32_t i = i0; i < nl; i += kBatch * step) {
-    uint32_t cc[kBatch];
-    Acc vv[kBatch];
-    double ac[kBatch];
+  for (uint32_t i = i0; i < nl; i += NB * step) {
+    uint32_t cc[NB];
+    Acc vv[NB];
+    double ac[NB];
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
+    for (int k = 0; k < NB; ++k) {
       const uint32_t ik = i + k * step;
       cc[k] = kEmpty;
       vv[k] = Acc(0);
@@ -477,9 +477,9 @@ __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxC
       if (cc[k] == x.cv) cc[k] = kEmpty;
     }
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
+    for (int k = 0; k < NB; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
+    for (int k = 0; k < NB; ++k) {
       if (cc[k] == kEmpty) continue;
       const float diff = __fsub_rn(Tr::to_float(vv[k]), self_v);
       const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
@@ -552,10 +552,20 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
       uint32_t nl = 0;
-      if (live) nl = insert_list<WINT, false>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+      // a row of at most T entries gives each lane at most one entry and one listed key:
+      // no batching then (team-uniform choice)
+      const bool one = x.re - x.rs <= (uint32_t)T;
+      if (live) {
+        if (one) nl = insert_list<WINT, false, 1>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+        else nl = insert_list<WINT, false, kBatch>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+      }
       self_acc = team_sum<T>(self_acc);
       __syncwarp();
-      if (live) best = list_scan<WINT>(D, x, tbl, list, lane, nl, T, Tr::to_float(self_acc), lowest);
+      if (live) {
+        const float self_v = Tr::to_float(self_acc);
+        if (one) best = list_scan<WINT, 1>(D, x, tbl, list, lane, nl, T, self_v, lowest);
+        else best = list_scan<WINT, kBatch>(D, x, tbl, list, lane, nl, T, self_v, lowest);
+      }
       best = team_max<T>(best, kFull);
       __syncwarp();  // the listed slots are empty again before the next vertex inserts
     }
@@ -653,10 +663,10 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
       if (threadIdx.x == 0) nlist = 0;
       __syncthreads();  // the table is empty and the list count zero
-      if (ok) insert_list<WINT, true>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist, self_acc, err);
+      if (ok) insert_list<WINT, true, kBatch>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist, self_acc, err);
       self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));  // (its barriers order the list)
       const uint32_t nl = nlist;
-      if (ok) best = list_scan<WINT>(D, x, tbl, list, threadIdx.x, nl, NT, Tr::to_float(self_acc), lowest);
+      if (ok) best = list_scan<WINT, kBatch>(D, x, tbl, list, threadIdx.x, nl, NT, Tr::to_float(self_acc), lowest);
     }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best) {
@@ -674,6 +684,50 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
 // evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
 // atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
 // Global tables are packed (key << 32 | sum) with integer weights, split arrays with fp32 ones.
+// Insert half for a global packed table (integer weights): the kBatch entries of a lane first
+// try their home slots with independent CAS operations, all in flight at once (nearly every
+// entry of a long row lands on a community not yet in the table, so the CAS usually creates
+// the key); an entry whose home slot holds its key adds to it, one whose home slot holds
+// another key probes on from there as PackedTable::add does.
+__device__ __forceinline__ void insert_scan_global(const Dev& D, const VtxCtx& x, uint32_t v,
+                                                   uint32_t e0, uint32_t step, const PackedTable& tbl,
+                                                   uint32_t& self_acc, uint32_t& err) {
+  const uint32_t* __restrict__ w = reinterpret_cast<const uint32_t*>(D.w);
+  for (uint32_t e = e0; e < x.re; e += kBatch * step) {
+    uint32_t uu[kBatch], cc[kBatch], ww[kBatch], hh[kBatch];
+    unsigned long long old[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const uint32_t ek = e + k * step;
+      const bool in = ek < x.re;
+      uu[k] = in ? D.col[ek] : v;
+      ww[k] = in ? (x.unit ? 1u : w[ek]) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      old[k] = kEmptySlot;
+      if (cc[k] != kEmpty && cc[k] != x.cv) {
+        hh[k] = hash_slot(cc[k], tbl.shift);
+        old[k] = atomicCAS(&tbl.slots[hh[k]], kEmptySlot, ((unsigned long long)cc[k] << 32) | ww[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (cc[k] == kEmpty) continue;
+      if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
+      if (old[k] == kEmptySlot) continue;  // created with its weight
+      if ((uint32_t)(old[k] >> 32) == cc[k]) {
+        atomicAdd(&tbl.slots[hh[k]], (unsigned long long)ww[k]);
+        continue;
+      }
+      const PackedTable rest{tbl.slots, tbl.mask, tbl.shift};
+      if (!rest.add_from((hh[k] + 1) & tbl.mask, cc[k], ww[k])) err |= kErrTableFull;
+    }
+  }
+}
+
 template <bool WINT>
 __device__ __forceinline__ void arena_clear_slot(const Dev& D, uint32_t s) {
   unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
@@ -734,7 +788,7 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
         if constexpr (WINT) {
           const PackedTable tbl{reinterpret_cast<unsigned long long*>(D.arena_vals) + off, cap - 1u,
                                 32u - log2_pow2(cap)};
-          insert_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x, tbl, self_acc, err);
+          insert_scan_global(D, x, v, pstart + threadIdx.x, blockDim.x, tbl, self_acc, err);
         } else {
           const SplitTable<Acc> tbl{D.arena_keys + off, reinterpret_cast<Acc*>(D.arena_vals) + off,
                                     cap - 1u, 32u - log2_pow2(cap)};
@@ -1819,6 +1873,7 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
   Ctrl* C = D.ctrl;
   const uint32_t count = C->long_count;
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
+  const bool unit = unit_weights<WINT>(C);
   uint32_t err = 0;
   const uint32_t n = C->n, n2 = C->n_next;
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
@@ -1837,10 +1892,49 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
     const uint32_t rs = D.row[v] + piece * kHubInsPiece;
     const uint32_t re = min(D.row[v + 1], rs + kHubInsPiece);
     Acc self_acc = Acc(0);
-    for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
-      const uint32_t d = D.new_comm[D.col[e]];
-      if (d == s) { self_acc += (Acc)w[e]; continue; }
-      if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
+    if constexpr (WINT) {
+      // kBatch entries per thread: their destinations, communities and home-slot CAS
+      // operations are each issued together; a home slot holding the key is added to, one
+      // holding another key is probed on from (PackedTable::add_from)
+      const PackedTable tbl{reinterpret_cast<unsigned long long*>(D.arena_vals) + off, cap - 1u,
+                            32u - log2_pow2(cap)};
+      for (uint32_t e = rs + threadIdx.x; e < re; e += kBatch * blockDim.x) {
+        uint32_t dd[kBatch], ww[kBatch], hh[kBatch];
+        unsigned long long old[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          const uint32_t ek = e + k * blockDim.x;
+          dd[k] = ek < re ? D.col[ek] : kEmpty;
+          ww[k] = ek < re ? (unit ? 1u : (uint32_t)w[ek]) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) dd[k] = dd[k] != kEmpty ? D.new_comm[dd[k]] : kEmpty;
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          old[k] = kEmptySlot;
+          if (dd[k] != kEmpty && dd[k] != s) {
+            hh[k] = hash_slot(dd[k], tbl.shift);
+            old[k] = atomicCAS(&tbl.slots[hh[k]], kEmptySlot, ((unsigned long long)dd[k] << 32) | ww[k]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          if (dd[k] == kEmpty) continue;
+          if (dd[k] == s) { self_acc += (Acc)ww[k]; continue; }
+          if (old[k] == kEmptySlot) continue;
+          if ((uint32_t)(old[k] >> 32) == dd[k]) {
+            atomicAdd(&tbl.slots[hh[k]], (unsigned long long)ww[k]);
+          } else if (!tbl.add_from((hh[k] + 1) & tbl.mask, dd[k], ww[k])) {
+            err |= kErrTableFull;
+          }
+        }
+      }
+    } else {
+      for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
+        const uint32_t d = D.new_comm[D.col[e]];
+        if (d == s) { self_acc += (Acc)w[e]; continue; }
+        if (!hub_table_add<WINT>(D, off, cap, d, (Acc)w[e])) err |= kErrTableFull;
+      }
     }
     self_acc = block_sum<256>(self_acc, sh);
     if (threadIdx.x == 0 && self_acc != Acc(0)) {
