@@ -437,6 +437,32 @@ __device__ __forceinline__ void warp_expand_rows(uint32_t rs, uint32_t len, uint
   }
 }
 
+// warp_expand_rows that calls f(entry index, valid) on every lane in every step (lanes past
+// the last entry with valid = false), so that f may use warp-wide votes.
+template <class F>
+__device__ __forceinline__ void warp_expand_rows_all(uint32_t rs, uint32_t len, F&& f) {
+  const int lane = threadIdx.x & 31;
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t excl = incl - len;
+  for (uint32_t jb = 0; jb < total; jb += 32) {
+    const uint32_t j = jb + lane;
+    int k = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const uint32_t ex = __shfl_sync(kFull, excl, k + step);
+      if (ex <= j) k += step;
+    }
+    const uint32_t base = __shfl_sync(kFull, rs, k) - __shfl_sync(kFull, excl, k);
+    f(base + j, j < total);
+  }
+}
+
 // The same with three payload words per row: f(entry index, pa, pb, pc).
 template <class F>
 __device__ __forceinline__ void warp_expand_rows3(uint32_t rs, uint32_t len, uint32_t pa, uint32_t pb,

@@ -346,9 +346,9 @@ class Run {
         throw Fail{LV_ERR_ARGUMENT, "team bin table does not fit shared memory"};
   }
 
-  // Shared memory per table slot: the contraction's tables (key + sum) and the gain kernels'
-  // (key + sum, plus half a u16 of key list per slot: the list holds cap / 2 slot indices).
-  size_t con_slot_bytes() const { return 4 + acc_size(); }
+  // Shared memory per table slot of the gain and contraction kernels: key + sum, plus half a
+  // u16 of key list per slot (the list holds cap / 2 slot indices).
+  size_t con_slot_bytes() const { return 4 + acc_size() + 1; }
   size_t opt_slot_bytes() const { return 4 + acc_size() + 1; }
 
   template <int T>
@@ -850,7 +850,7 @@ class Run {
   }
   template <bool WI>
   void agg_contract_b() {
-    const size_t slot = 4 + (WI ? 4 : 8);
+    const size_t slot = con_slot_bytes();
     // the largest new communities: many blocks insert into their global tables
     k_arena_clear<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_hub_owner<<<ctx->sms * 2, 256, 0, st>>>(Dd, kNumBins - 1);

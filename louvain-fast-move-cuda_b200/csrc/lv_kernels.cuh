@@ -2049,14 +2049,25 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
   constexpr int TEAMS = 256 / T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int team = threadIdx.x / T, lane = threadIdx.x % T;
+  // per team: a table of `cap` slots and a list of cap / 2 u16 slot indices (as k_opt_team)
+  constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
+  unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
+  uint16_t* klist = reinterpret_cast<uint16_t*>(smem + (size_t)TEAMS * cap * kSlotBytes) + (size_t)team * (cap / 2);
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
+  if (blockIdx.x * TEAMS >= count) return;  // (block-uniform)
   const uint32_t* list = D.bins[bin];
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
+  const bool unit = unit_weights<WINT>(C);
+  const unsigned tmask = T == 32 ? kFull : (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(uint32_t)(T - 1)));
+  const uint32_t lt = lanemask_lt();
   uint32_t err = 0;
+  ScratchTable<WINT> tbl{keys, vals, slots, cap - 1u, 0u};
+  for (uint32_t i = lane; i < cap; i += T) tbl.clear(i);
+  __syncwarp();
   for (uint32_t base = blockIdx.x * TEAMS; base < count; base += gridDim.x * TEAMS) {
     const uint32_t idx = base + team;
     const bool live = idx < count;
@@ -2064,18 +2075,30 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     CommCtx x{};
     if (live) x = load_comm(D, s);
     const uint32_t cap_v = live ? contract_cap(x.dsum, D.gs[x.g].n_next, false) : 2u;
-    const ScratchTable<WINT> tbl{keys, vals, reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap,
-                                 cap_v - 1u, 32u - log2_pow2(cap_v)};
-    if (live)
-      for (uint32_t i = lane; i < cap_v; i += T) tbl.clear(i);
-    __syncwarp();
+    tbl.mask = cap_v - 1u;
+    tbl.shift = 32u - log2_pow2(cap_v);
     // entries staying inside the community (the new self-loop, the hottest key) are summed in
-    // registers; only entries to other communities go through the table
+    // registers; only entries to other communities go through the table, and each community
+    // the table gains is listed
     Acc self_acc = Acc(0);
-    auto add = [&](uint32_t e, uint32_t, uint32_t) {
-      const uint32_t d = D.new_comm[D.col[e]];
-      if (d == s) { self_acc += (Acc)w[e]; return; }
-      if (!tbl.add(d, (Acc)w[e])) err |= kErrTableFull;
+    uint32_t nl = 0;
+    auto add = [&](uint32_t e, bool valid) {
+      bool made = false;
+      uint32_t slot = 0;
+      if (valid) {
+        const uint32_t d = D.new_comm[D.col[e]];
+        const Acc wv = unit ? Acc(1) : (Acc)w[e];
+        if (d == s) {
+          self_acc += wv;
+        } else {
+          const int r = tbl.add_at(d, wv, slot);
+          if (!r) err |= kErrTableFull;
+          made = r == 2;
+        }
+      }
+      const unsigned m = __ballot_sync(tmask, made) & tmask;
+      if (made) klist[nl + __popc(m & lt)] = (uint16_t)slot;
+      nl += __popc(m);
     };
     if (T == 32) {
       // a warp per community: members taken 32 at a time, their entries spread over all lanes
@@ -2087,48 +2110,32 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
             rs = D.row[v];
             len = D.row[v + 1] - rs;
           }
-          warp_expand_rows(rs, len, 0u, 0u, add);
+          warp_expand_rows_all(rs, len, add);
         }
       }
     } else if (live) {
       for (uint32_t i = x.mb; i < x.me; ++i) {
         const uint32_t v = D.members[i];
         const uint32_t re = D.row[v + 1];
-        for (uint32_t e = D.row[v] + lane; e < re; e += T) add(e, 0u, 0u);
+        for (uint32_t eb = D.row[v]; eb < re; eb += T) add(eb + lane, eb + lane < re);
       }
     }
     self_acc = team_sum<T>(self_acc);
     __syncwarp();
-    // compact the occupied slots of this team's table into the output row
-    uint32_t cnt = 0;
+    // the listed communities become the output row, in list order; their slots are emptied
     double ksum = 0.0;
-    if (live)
-      for (uint32_t i = lane; i < cap_v; i += T) {
-        uint32_t d;
-        Acc sum;
-        tbl.load(i, d, sum);
-        cnt += d != kEmpty;
-      }
-    uint32_t off = cnt;
-#pragma unroll
-    for (int o = 1; o < T; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(kFull, off, o, T);
-      if (lane >= o) off += y;
-    }
-    const uint32_t total = __shfl_sync(kFull, off, T - 1, T);
-    off -= cnt;
     if (live) {
-      for (uint32_t i = lane; i < cap_v; i += T) {
+      for (uint32_t i = lane; i < nl; i += T) {
+        const uint32_t sl = klist[i];
         uint32_t d;
         Acc sum;
-        tbl.load(i, d, sum);
-        if (d == kEmpty) continue;
+        tbl.load(sl, d, sum);
+        tbl.clear(sl);
         Wt wv;
         if (WINT) wv = (Wt)sum;
         else wv = (Wt)__double2float_rn((double)sum);
-        D.colB[x.tb + off] = d;
-        wout[x.tb + off] = wv;
-        ++off;
+        D.colB[x.tb + i] = d;
+        wout[x.tb + i] = wv;
         ksum += Tr::w_double(wv);
       }
     }
@@ -2140,13 +2147,13 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
         Wt wv;
         if (WINT) wv = (Wt)self_acc;
         else wv = (Wt)__double2float_rn((double)self_acc);
-        D.colB[x.tb + total] = s;
-        wout[x.tb + total] = wv;
+        D.colB[x.tb + nl] = s;
+        wout[x.tb + nl] = wv;
         ksum += Tr::w_double(wv);
         if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
         else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), Tr::w_double(wv));
       }
-      D.newdeg[s] = total + (has_self ? 1u : 0u);
+      D.newdeg[s] = nl + (has_self ? 1u : 0u);
       D.kB[s] = ksum;
       if (D.gidB) D.gidB[s] = x.g;
     }
@@ -2155,7 +2162,7 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
   if (err) atomicOr(&C->err, err);
 }
 
-// One block per new community of bin 6 (shared-memory table).
+// One block per new community of bin 6 (shared-memory table, listed keys as above).
 template <bool WINT>
 __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
@@ -2167,32 +2174,35 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
   __shared__ uint32_t shu[33];
   __shared__ double shd[33];
   __shared__ uint32_t mrs[NT], mex[NT];  // row start / entry offset of the members in flight
+  __shared__ uint32_t nlist;
+  constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
+  uint16_t* klist = reinterpret_cast<uint16_t*>(smem + (size_t)cap * kSlotBytes);
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
+  if (blockIdx.x >= count) return;  // (block-uniform)
   const uint32_t* list = D.bins[bin];
   const Wt* __restrict__ w = reinterpret_cast<const Wt*>(D.w);
   Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.wB);
+  const bool unit = unit_weights<WINT>(C);
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = lanemask_lt();
   uint32_t err = 0;
+  ScratchTable<WINT> tbl{reinterpret_cast<uint32_t*>(smem),
+                         reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t)),
+                         reinterpret_cast<unsigned long long*>(smem), cap - 1u, 0u};
+  for (uint32_t i = threadIdx.x; i < cap; i += NT) tbl.clear(i);
   for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
     const uint32_t s = list[idx];
     const CommCtx x = load_comm(D, s);
     const uint32_t cap_v = contract_cap(x.dsum, D.gs[x.g].n_next, false);
     const bool ok = cap_v <= cap;
-    const ScratchTable<WINT> tbl{reinterpret_cast<uint32_t*>(smem),
-                                 reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t)),
-                                 reinterpret_cast<unsigned long long*>(smem), cap_v - 1u,
-                                 32u - log2_pow2(cap_v)};
+    tbl.mask = cap_v - 1u;
+    tbl.shift = 32u - log2_pow2(cap_v);
     if (!ok) err |= kErrArena;
-    if (ok)
-      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) tbl.clear(i);
-    __syncthreads();
+    if (threadIdx.x == 0) nlist = 0;
+    __syncthreads();  // the table is empty and the list count zero
     Acc self_acc = Acc(0);  // entries staying inside the community, kept out of the table
     if (ok) {
-      auto add = [&](uint32_t e, uint32_t, uint32_t) {
-        const uint32_t d = D.new_comm[D.col[e]];
-        if (d == s) { self_acc += (Acc)w[e]; return; }
-        if (!tbl.add(d, (Acc)w[e])) err |= kErrTableFull;
-      };
       // members taken NT at a time; their entries spread evenly over the whole block, each
       // thread finding its entry's member by binary search in shared memory
       for (uint32_t base = x.mb; base < x.me; base += NT) {
@@ -2209,41 +2219,54 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
         mex[threadIdx.x] = ex;
         __syncthreads();
         const uint32_t cnt = min((uint32_t)NT, x.me - base);
-        for (uint32_t j = threadIdx.x; j < total; j += NT) {
-          uint32_t lo = 0, hi = cnt;
-          while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (mex[mid] <= j) lo = mid; else hi = mid;
+        for (uint32_t jb = 0; jb < total; jb += NT) {
+          const uint32_t j = jb + threadIdx.x;
+          bool made = false;
+          uint32_t slot = 0;
+          if (j < total) {
+            uint32_t lo = 0, hi = cnt;
+            while (hi - lo > 1) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (mex[mid] <= j) lo = mid; else hi = mid;
+            }
+            const uint32_t e = mrs[lo] + (j - mex[lo]);
+            const uint32_t d = D.new_comm[D.col[e]];
+            const Acc wv = unit ? Acc(1) : (Acc)w[e];
+            if (d == s) {
+              self_acc += wv;
+            } else {
+              const int r = tbl.add_at(d, wv, slot);
+              if (!r) err |= kErrTableFull;
+              made = r == 2;
+            }
           }
-          add(mrs[lo] + (j - mex[lo]), 0u, 0u);
+          const unsigned m = __ballot_sync(kFull, made);
+          if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t b0 = 0;
+            if (lane == leader) b0 = atomicAdd(&nlist, (uint32_t)__popc(m));
+            b0 = __shfl_sync(kFull, b0, leader);
+            if (made) klist[b0 + __popc(m & lt)] = (uint16_t)slot;
+          }
         }
         __syncthreads();
       }
     }
-    self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(shd));
-    uint32_t cnt = 0;
-    if (ok)
-      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) {
-        uint32_t d;
-        Acc sum;
-        tbl.load(i, d, sum);
-        cnt += d != kEmpty;
-      }
-    uint32_t total;
-    uint32_t off = block_excl_scan<uint32_t, NT>(cnt, shu, &total);
+    self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(shd));  // (its barriers order the list)
+    const uint32_t nl = nlist;
     double ksum = 0.0;
     if (ok) {
-      for (uint32_t i = threadIdx.x; i < cap_v; i += NT) {
+      for (uint32_t i = threadIdx.x; i < nl; i += NT) {
+        const uint32_t sl = klist[i];
         uint32_t d;
         Acc sum;
-        tbl.load(i, d, sum);
-        if (d == kEmpty) continue;
+        tbl.load(sl, d, sum);
+        tbl.clear(sl);
         Wt wv;
         if (WINT) wv = (Wt)sum;
         else wv = (Wt)__double2float_rn((double)sum);
-        D.colB[x.tb + off] = d;
-        wout[x.tb + off] = wv;
-        ++off;
+        D.colB[x.tb + i] = d;
+        wout[x.tb + i] = wv;
         ksum += Tr::w_double(wv);
       }
     }
@@ -2255,13 +2278,13 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
         Wt wv;
         if (WINT) wv = (Wt)self_acc;
         else wv = (Wt)__double2float_rn((double)self_acc);
-        D.colB[x.tb + total] = s;
-        wout[x.tb + total] = wv;
+        D.colB[x.tb + nl] = s;
+        wout[x.tb + nl] = wv;
         ktot += Tr::w_double(wv);
         if (WINT) atomicAdd(&D.gs[x.g].I, (unsigned long long)wv);
         else atomicAdd(reinterpret_cast<double*>(&D.gs[x.g].I), Tr::w_double(wv));
       }
-      D.newdeg[s] = ok ? total + (has_self ? 1u : 0u) : 0u;
+      D.newdeg[s] = ok ? nl + (has_self ? 1u : 0u) : 0u;
       D.kB[s] = ktot;
       if (D.gidB) D.gidB[s] = x.g;
     }
