@@ -336,17 +336,15 @@ struct PackedTable {
     k = (uint32_t)(x >> 32);
     v = (uint32_t)x;
   }
-  // add() that reports the slot and whether this call created the key (as table_add_at)
+  // add() that reports the slot and whether this call created the key (as table_add_at). It
+  // tries the CAS first, without reading the slot before: almost every insert of a gain pass
+  // creates its key, and a CAS that fails returns the slot's content anyway.
   __device__ __forceinline__ int add_at(uint32_t c, uint32_t w, uint32_t& slot) const {
     uint32_t h = hash_slot(c, shift);
     for (uint32_t probe = 0; probe <= mask; ++probe) {
-      unsigned long long cur = ((volatile unsigned long long*)slots)[h];
-      uint32_t key = (uint32_t)(cur >> 32);
-      if (key == kEmpty) {
-        cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
-        if (cur == kEmptySlot) { slot = h; return 2; }
-        key = (uint32_t)(cur >> 32);
-      }
+      const unsigned long long cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
+      if (cur == kEmptySlot) { slot = h; return 2; }
+      const uint32_t key = (uint32_t)(cur >> 32);
       if (key == c) {
         atomicAdd(&slots[h], (unsigned long long)w);
         slot = h;

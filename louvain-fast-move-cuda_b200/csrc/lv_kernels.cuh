@@ -493,6 +493,12 @@ __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxC
   return best;
 }
 
+// Entries per thread and step for a row of d entries over `lanes` lanes: as many as the row
+// needs, up to kBatch (unused batch slots still cost their instructions).
+__device__ __forceinline__ int batch_for(uint32_t d, uint32_t lanes) {
+  return d <= lanes ? 1 : (d <= 2u * lanes ? 2 : kBatch);
+}
+
 // ---- pass: optimisation, one team of T lanes per vertex -----------------------------------------
 // Fast pass (iteration 0 of a level, phaseOptimizationSort.cu:28-158): per-entry gains with
 // self = 0 and the destination's own (singleton) community, argmax over positive gains with
@@ -552,18 +558,20 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
       // weight into the vertex's own community stays in registers (it is the hottest key)
       Acc self_acc = Acc(0);
       uint32_t nl = 0;
-      // a row of at most T entries gives each lane at most one entry and one listed key:
-      // no batching then (team-uniform choice)
-      const bool one = x.re - x.rs <= (uint32_t)T;
+      // entries per lane and step as the row needs (team-uniform choice): unused batch slots
+      // still cost their instructions
+      const int nb = batch_for(x.re - x.rs, T);
       if (live) {
-        if (one) nl = insert_list<WINT, false, 1>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+        if (nb == 1) nl = insert_list<WINT, false, 1>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+        else if (nb == 2) nl = insert_list<WINT, false, 2>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
         else nl = insert_list<WINT, false, kBatch>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
       }
       self_acc = team_sum<T>(self_acc);
       __syncwarp();
       if (live) {
         const float self_v = Tr::to_float(self_acc);
-        if (one) best = list_scan<WINT, 1>(D, x, tbl, list, lane, nl, T, self_v, lowest);
+        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, lane, nl, T, self_v, lowest);
+        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, lane, nl, T, self_v, lowest);
         else best = list_scan<WINT, kBatch>(D, x, tbl, list, lane, nl, T, self_v, lowest);
       }
       best = team_max<T>(best, kFull);
@@ -621,14 +629,18 @@ __device__ __forceinline__ unsigned long long block_max(unsigned long long x, un
 // The vertex's table lives in shared memory (capacity `cap` slots; vertices whose table would
 // not fit are in bin 7, handled by the k_opt_hub_* kernels).
 template <bool WINT>
-__global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t cap) {
+__global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
-  constexpr int NT = 512;
+  constexpr int NT = 512, NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ unsigned long long red[33];
-  __shared__ uint32_t nlist;
+  // per-warp partials and the list count, double-buffered by vertex parity so that a vertex
+  // needs two barriers (table pass) or one (fast pass): one before the keys are evaluated,
+  // one before warp 0 reads the per-warp best keys
+  __shared__ unsigned long long red_best[2][NW];
+  __shared__ Acc red_self[2][NW];
+  __shared__ uint32_t nlist[2];
   // a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 u16 slot indices
   constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
@@ -643,37 +655,61 @@ __global__ void __launch_bounds__(512) k_opt_block(int dslot, int bin, uint32_t 
   const bool fast = C->fast != 0;
   const bool lowest = fast || C->rule_sort != 0;
   const bool unit = unit_weights<WINT>(C);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t err = 0;
   ScratchTable<WINT> tbl{keys, vals, slots, cap - 1u, 0u};
   if (!fast)
     for (uint32_t s = threadIdx.x; s < cap; s += NT) tbl.clear(s);
+  if (threadIdx.x < 2) nlist[threadIdx.x] = 0;
+  __syncthreads();
 
-  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+  int par = 0;
+  for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x, par ^= 1) {
     const uint32_t v = vlist[idx];
     const VtxCtx x = load_vtx(D, v, unit);
+    const uint32_t d = x.re - x.rs;
+    const int nb = batch_for(d, NT);
     unsigned long long best = 0;
     if (fast) {
       best = fast_scan<WINT>(D, x, v, x.rs + threadIdx.x, NT);
     } else {
-      const uint32_t cap_v = table_cap(x.re - x.rs, x.ng);
+      const uint32_t cap_v = table_cap(d, x.ng);
       const bool ok = cap_v <= cap;
       if (!ok) err |= kErrArena;
       tbl.mask = cap_v - 1u;
       tbl.shift = 32u - log2_pow2(cap_v);
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
-      if (threadIdx.x == 0) nlist = 0;
-      __syncthreads();  // the table is empty and the list count zero
-      if (ok) insert_list<WINT, true, kBatch>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist, self_acc, err);
-      self_acc = block_sum<NT>(self_acc, reinterpret_cast<Acc*>(red));  // (its barriers order the list)
-      const uint32_t nl = nlist;
-      if (ok) best = list_scan<WINT, kBatch>(D, x, tbl, list, threadIdx.x, nl, NT, Tr::to_float(self_acc), lowest);
+      if (ok) {
+        if (nb == 1) insert_list<WINT, true, 1>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
+        else if (nb == 2) insert_list<WINT, true, 2>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
+        else insert_list<WINT, true, kBatch>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
+      }
+      self_acc = warp_sum(self_acc);
+      if (lane == 0) red_self[par][wid] = self_acc;
+      __syncthreads();  // the table and the list are complete
+      Acc self_all = Acc(0);
+#pragma unroll
+      for (int i = 0; i < NW; ++i) self_all += red_self[par][i];  // fixed order
+      const uint32_t nl = nlist[par];
+      const float self_v = Tr::to_float(self_all);
+      if (ok) {
+        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
+        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
+        else best = list_scan<WINT, kBatch>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
+      }
+      if (threadIdx.x == 0) nlist[par ^ 1] = 0;  // the next vertex's count (read by no one now)
     }
-    best = block_max<NT>(best, red);
-    if (threadIdx.x == 0 && best) {
-      const uint32_t c = key_comm(best, lowest);
-      if (c != x.cv && (!fast || v <= c)) emit_hub_move(D, v, c, it, x.re - x.rs);
+    best = team_max<32>(best, kFull);
+    if (lane == 0) red_best[par][wid] = best;
+    __syncthreads();  // every key is evaluated and every listed slot empty again
+    if (wid == 0) {
+      unsigned long long y = lane < NW ? red_best[par][lane] : 0ull;
+      y = team_max<32>(y, kFull);
+      if (lane == 0 && y) {
+        const uint32_t c = key_comm(y, lowest);
+        if (c != x.cv && (!fast || v <= c)) emit_hub_move(D, v, c, it, d);
+      }
     }
-    __syncthreads();
   }
   if (err) atomicOr(&C->err, err);
 }
