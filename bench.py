@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--cpu-sample-scale", type=int, default=21)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-loop", action="store_true",
-                    help="served: also time the reference's CUDA build once per pool graph")
+                    help="batched / served: also time the reference's CUDA build once per graph "
+                         "(served: the whole pool; batched: every 64th graph)")
     ap.add_argument("--no-summaries", action="store_true",
                     help="skip the compact batched / served records of the default line")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -395,6 +396,15 @@ def run_batched(args, local, emit=True):
     loop_ms = (time.perf_counter() - t0) * 1e3
     offs = b.vtx_offsets.cpu().numpy()
     same = all(torch.equal(out_d[offs[g]: offs[g + 1]], outs[g]) for g in range(b.G))
+    ref_loop = None
+    if args.reference_loop:
+        # the reference's own loop on every 64th graph (a log-uniform sample of the sizes)
+        graphs_mod = importlib.import_module(PKG + ".graphs")
+        sample = [graphs_mod.CSRGraph(n=n, row_ptr=rp.cpu().numpy().astype(np.int64), col=cl.cpu().numpy())
+                  for n, rp, cl in singles[::64]]
+        ref_loop = reference_loop(sample, args)
+        if ref_loop.get("graphs") is not None:
+            ref_loop["sample"] = f"every 64th graph of the batch ({len(sample)} graphs)"
     m_total = int(b.m.sum())
     line = {
         "metric": "batched_graphs_per_s", "value": b.G / (batch_ms / 1e3), "unit": "graphs/s",
@@ -408,6 +418,9 @@ def run_batched(args, local, emit=True):
         "loop": {"graphs_per_s": b.G / (loop_ms / 1e3), "ms": loop_ms, "gpu_launches": int(loop_launches),
                  "what": "one lv_run_csr call per graph, device-resident inputs, same engine"},
         "speedup_vs_loop": loop_ms / batch_ms,
+        "reference_loop": ref_loop,
+        "speedup_vs_reference_loop": (b.G / (batch_ms / 1e3) / ref_loop["graphs_per_s"]
+                                      if ref_loop and ref_loop.get("graphs_per_s") else None),
         "parity": {"partitions_equal": bool(same),
                    "max_abs_dq": float(np.max(np.abs(np.asarray(qs) - q_loop)))},
         "levels": st.levels, "passes": st.iterations, "gpu_launches": int(launches),
@@ -495,25 +508,29 @@ def run_served(args, local, emit=True):
             else:
                 which = rng.integers(0, len(pool), n_req)
             gaps = rng.exponential(1.0 / rate, n_req)
-            ids, lat = {}, []
+            # the submitter only submits, at the Poisson arrival times; completion times come
+            # from the server's own clock (latency = done - submit), read after the stream ends,
+            # so that polling never competes with the workers for the server's lock
+            sub_t, ids = [], []
             t_start = time.perf_counter()
             t_next = t_start
-            i = 0
-            done_t = None
-            while i < n_req or ids:
-                now = time.perf_counter()
-                while i < n_req and now >= t_next:
-                    ids[srv.submit(pool[which[i]], borrow=True)] = which[i]
-                    t_next += gaps[i]
-                    i += 1
-                for rid in list(ids):
-                    r = srv.poll(rid)
-                    if r is not None:
-                        lat.append(r[2])
-                        worst_dq = max(worst_dq, abs(r[1] - ref_q[ids.pop(rid)]))
-                        done_t = time.perf_counter()
-                time.sleep(0.0002)
-            span = done_t - t_start
+            for i in range(n_req):
+                while True:
+                    now = time.perf_counter()
+                    if now >= t_next:
+                        break
+                    time.sleep(min(0.0005, t_next - now))
+                sub_t.append(time.perf_counter())
+                ids.append((srv.submit(pool[which[i]], borrow=True), which[i]))
+                t_next += gaps[i]
+            srv.drain()
+            lat, ends = [], []
+            for (rid, gi), ts in zip(ids, sub_t):
+                r = srv.poll(rid)
+                lat.append(r[2])
+                ends.append(ts + r[2] / 1e3)
+                worst_dq = max(worst_dq, abs(r[1] - ref_q[gi]))
+            span = max(ends) - t_start
             rates.append({"rate": rate, "requests": n_req, "graphs_per_s": n_req / span,
                           "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99)})
     best = max(rates, key=lambda r: r["graphs_per_s"])
@@ -532,6 +549,8 @@ def run_served(args, local, emit=True):
         "speedup_vs_loop": best["graphs_per_s"] / loop_gps,
         "parity": {"max_abs_dq_vs_alone": worst_dq},
         "reference_loop": ref_loop,
+        "speedup_vs_reference_loop": (best["graphs_per_s"] / ref_loop["graphs_per_s"]
+                                      if ref_loop and ref_loop.get("graphs_per_s") else None),
         "clocks": clk.summary(),
         "autotune": tune,
     }
@@ -602,9 +621,10 @@ def system_summaries(args, local):
     stream at its saturated rate (2,000 requests/s, pool of 64) against its loop."""
     out = {}
     for name, fn, over in (
-            ("batched", run_batched, {"steps": 2, "warmup": 1, "graphs": 4096, "no_autotune": True}),
+            ("batched", run_batched, {"steps": 2, "warmup": 1, "graphs": 4096, "no_autotune": True,
+                                      "reference_loop": True}),
             ("served", run_served, {"rates": "2000", "pool": 64, "slots": 16, "no_autotune": True,
-                                    "captured": -1})):
+                                    "captured": -1, "reference_loop": True})):
         a = argparse.Namespace(**vars(args))
         for k, v in over.items():
             setattr(a, k, v)
@@ -617,6 +637,8 @@ def system_summaries(args, local):
             out[name] = {"graphs_per_s": r["value"], "ms_per_batch": r["ms_per_step"],
                          "loop_graphs_per_s": r["loop"]["graphs_per_s"],
                          "speedup_vs_loop": r["speedup_vs_loop"], "parity": r["parity"],
+                         "reference_loop": r["reference_loop"],
+                         "speedup_vs_reference_loop": r["speedup_vs_reference_loop"],
                          "config": r["config"], "steps": a.steps, "warmup": a.warmup}
         else:
             rr = r["rates"][0]
@@ -624,6 +646,8 @@ def system_summaries(args, local):
                          "p99_ms": rr["p99_ms"], "rate": rr["rate"], "requests": rr["requests"],
                          "loop_graphs_per_s": r["loop"]["graphs_per_s"],
                          "speedup_vs_loop": r["speedup_vs_loop"], "parity": r["parity"],
+                         "reference_loop": r["reference_loop"],
+                         "speedup_vs_reference_loop": r["speedup_vs_reference_loop"],
                          "config": r["config"]}
     return out
 

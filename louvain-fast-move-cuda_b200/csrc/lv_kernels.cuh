@@ -99,6 +99,13 @@ __device__ __forceinline__ uint32_t hub_table_cap(uint32_t d, uint32_t ng) {
   return c < kHubChunk ? kHubChunk : c;
 }
 
+// Error bits found by a kernel, and which kernel found them (Ctrl::err_site, bit `site`), so
+// that a failed device check names the kernel.
+__device__ __forceinline__ void report_err(Ctrl* C, uint32_t err, int site) {
+  atomicOr(&C->err, err);
+  atomicOr(&C->err_site, 1u << site);
+}
+
 __device__ __forceinline__ int bin_of(const BinCfg& B, uint32_t d) {
 #pragma unroll
   for (int b = 0; b < kNumBins - 1; ++b)
@@ -585,7 +592,7 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
     }
     emit_move(D, move, v, c, it);
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 0);  // k_opt_team
 }
 
 // Block-wide sum (all threads call; result valid in every thread; `sh` holds >= 33 values).
@@ -711,7 +718,7 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
       }
     }
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 1);  // k_opt_block
 }
 
 // ---- pass: optimisation of the longest rows (bin 7), many blocks per vertex ------------------------
@@ -838,7 +845,7 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
       }
     }
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 2);  // k_opt_hub_scan
 }
 
 template <bool WINT>
@@ -1493,7 +1500,7 @@ __global__ void __launch_bounds__(256) k_prep(int dslot, const long long* row64,
   flush();
   if (err & kErrNotUnit) C->unit_w = 0;
   err &= ~kErrNotUnit;
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 3);  // k_prep
 }
 
 // Rows longer than kPrepLongRow entries, one block each.
@@ -1532,7 +1539,7 @@ __global__ void __launch_bounds__(512) k_prep_long(int dslot, const float* wf_in
   }
   if (err & kErrNotUnit) C->unit_w = 0;
   err &= ~kErrNotUnit;
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 4);  // k_prep_long
 }
 
 // m = (sum of k) / 2 per graph; integer mode requires 2m < 2^32 (the reference's u32 sums).
@@ -1895,7 +1902,7 @@ __global__ void __launch_bounds__(256) k_hub_insert(int dslot) {
     warp_expand_rows3(rs, len, s, off, cap, add);
   }
   flush_self();
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 5);  // k_hub_insert
 }
 
 // Pieces of the long rows deferred by k_hub_insert, one block per piece.
@@ -1978,7 +1985,7 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
       else atomicAdd(reinterpret_cast<double*>(&D.hubself[s]), (double)self_acc);
     }
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 6);  // k_hub_insert_long
 }
 
 // Bin-7 emit: one block per table chunk; occupied slots are appended to the community's row
@@ -2195,7 +2202,7 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
     }
     __syncwarp();
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 7);  // k_contract_team
 }
 
 // One block per new community of bin 6 (shared-memory table, listed keys as above).
@@ -2326,7 +2333,7 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
     }
     __syncthreads();
   }
-  if (err) atomicOr(&C->err, err);
+  if (err) report_err(C, err, 8);  // k_contract_block
 }
 
 // Copy the gapped contracted rows into the dense next-level CSR (col/w), move k' and gid'.
