@@ -83,6 +83,7 @@ struct Ctrl {
   uint32_t n_iterating;        // graphs still in kIterating after the last pass
   uint32_t err;
   uint32_t err_site;           // kernels that reported an error bit (one bit per reporting site)
+  unsigned long long err_info[2];  // the first failing check's own details (kernel-specific)
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
   uint32_t unit_w;             // integer mode, level 0: every weight is 1, so no kernel loads w

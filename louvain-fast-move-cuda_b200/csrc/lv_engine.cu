@@ -323,8 +323,13 @@ class Run {
     if (e & kErrInput) throw Fail{LV_ERR_INPUT, "input graph: a row is empty, a column index is outside its graph, or a weight is invalid for the weight mode"};
     if (e & kErrRange) throw Fail{LV_ERR_RANGE, "integer weights: total weight 2m must be below 2^32 (the reference sums in u32)"};
     if (e & kErrLoop) throw Fail{LV_ERR_DEVICE_CHECK, "captured run: pass or level guard tripped"};
-    if (e) throw Fail{LV_ERR_DEVICE_CHECK, "device check failed (flags " + std::to_string(e) + ", sites " +
-                                            std::to_string(ctrl_u32(offsetof(Ctrl, err_site))) + ")"};
+    if (e) {
+      const auto i0 = read_ctrl<unsigned long long>(offsetof(Ctrl, err_info));
+      const auto i1 = read_ctrl<unsigned long long>(offsetof(Ctrl, err_info) + 8);
+      throw Fail{LV_ERR_DEVICE_CHECK, "device check failed (flags " + std::to_string(e) + ", sites " +
+                                          std::to_string(ctrl_u32(offsetof(Ctrl, err_site))) + ", info " +
+                                          std::to_string(i0) + " " + std::to_string(i1) + ")"};
+    }
   }
 
   // ---- setup ------------------------------------------------------------------------------------

@@ -2241,7 +2241,12 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
     const bool ok = cap_v <= cap;
     tbl.mask = cap_v - 1u;
     tbl.shift = 32u - log2_pow2(cap_v);
-    if (!ok) err |= kErrArena;
+    if (!ok) {
+      err |= kErrArena;
+      if (threadIdx.x == 0 &&
+          atomicCAS(&C->err_info[0], 0ull, ((unsigned long long)s << 32) | x.dsum) == 0ull)
+        C->err_info[1] = ((unsigned long long)cap_v << 32) | cap;
+    }
     if (threadIdx.x == 0) nlist = 0;
     __syncthreads();  // the table is empty and the list count zero
     Acc self_acc = Acc(0);  // entries staying inside the community, kept out of the table
