@@ -315,6 +315,38 @@ struct PackedTable {
   __device__ __forceinline__ bool add(uint32_t c, uint32_t w) const {
     return add_from(hash_slot(c, shift), c, w);
   }
+  // NB inserts at once (entries with c[k] == kEmpty are skipped), each as add() does -- read
+  // the slot, CAS only an empty one, add to the own key, probe on past another key -- but with
+  // the NB home-slot reads issued together, then the NB CAS operations together, so that a
+  // lane waits for two memory round trips per batch instead of two per entry. Adds to an
+  // existing key do not wait for their result. Returns false if some entry found no slot.
+  template <int NB>
+  __device__ __forceinline__ bool add_batch(const uint32_t (&c)[NB], const uint32_t (&w)[NB]) const {
+    uint32_t h[NB];
+    unsigned long long cur[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      h[k] = hash_slot(c[k], shift);
+      cur[k] = c[k] != kEmpty ? ((volatile unsigned long long*)slots)[h[k]] : 0ull;
+    }
+    bool made[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      made[k] = false;
+      if (c[k] != kEmpty && cur[k] == kEmptySlot) {
+        cur[k] = atomicCAS(&slots[h[k]], kEmptySlot, ((unsigned long long)c[k] << 32) | w[k]);
+        made[k] = cur[k] == kEmptySlot;  // else cur holds what another insert put there
+      }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      if (c[k] == kEmpty || made[k]) continue;
+      if ((uint32_t)(cur[k] >> 32) == c[k]) atomicAdd(&slots[h[k]], (unsigned long long)w[k]);
+      else ok &= add_from((h[k] + 1) & mask, c[k], w[k]);
+    }
+    return ok;
+  }
   // add() with the probe sequence starting at slot h (the home slot, or one past it)
   __device__ __forceinline__ bool add_from(uint32_t h, uint32_t c, uint32_t w) const {
     for (uint32_t probe = 0; probe <= mask; ++probe) {
@@ -338,14 +370,26 @@ struct PackedTable {
     k = (uint32_t)(x >> 32);
     v = (uint32_t)x;
   }
-  // add() that reports the slot and whether this call created the key (as table_add_at). It
-  // tries the CAS first, without reading the slot before: almost every insert of a gain pass
-  // creates its key, and a CAS that fails returns the slot's content anyway.
+  // add() that reports the slot and whether this call created the key (as table_add_at).
+  // CAS_FIRST tries the CAS without reading the slot before: in a gain pass almost every insert
+  // creates its key (a row's neighbours sit in distinct communities), and a CAS that fails
+  // returns the slot's content anyway. Otherwise the slot is read first, which saves the failing
+  // CAS when keys repeat (contraction: a community's members share neighbouring communities).
+  template <bool CAS_FIRST = false>
   __device__ __forceinline__ int add_at(uint32_t c, uint32_t w, uint32_t& slot) const {
     uint32_t h = hash_slot(c, shift);
     for (uint32_t probe = 0; probe <= mask; ++probe) {
-      const unsigned long long cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
-      if (cur == kEmptySlot) { slot = h; return 2; }
+      unsigned long long cur;
+      if (CAS_FIRST) {
+        cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
+        if (cur == kEmptySlot) { slot = h; return 2; }
+      } else {
+        cur = ((volatile unsigned long long*)slots)[h];
+        if (cur == kEmptySlot) {
+          cur = atomicCAS(&slots[h], kEmptySlot, ((unsigned long long)c << 32) | w);
+          if (cur == kEmptySlot) { slot = h; return 2; }
+        }
+      }
       const uint32_t key = (uint32_t)(cur >> 32);
       if (key == c) {
         atomicAdd(&slots[h], (unsigned long long)w);
@@ -379,8 +423,9 @@ struct ScratchTable {
     if constexpr (WINT) return PackedTable{slots, mask, shift}.add(c, w);
     else return table_add(keys, vals, mask, shift, c, w);
   }
+  template <bool CAS_FIRST = false>
   __device__ __forceinline__ int add_at(uint32_t c, Acc w, uint32_t& slot) const {
-    if constexpr (WINT) return PackedTable{slots, mask, shift}.add_at(c, w, slot);
+    if constexpr (WINT) return PackedTable{slots, mask, shift}.template add_at<CAS_FIRST>(c, w, slot);
     else return table_add_at(keys, vals, mask, shift, c, w, slot);
   }
   __device__ __forceinline__ void load(uint32_t i, uint32_t& k, Acc& v) const {

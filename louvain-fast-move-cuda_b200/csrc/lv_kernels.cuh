@@ -435,7 +435,7 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
         if (cc[k] == x.cv) {
           self_acc += ww[k];
         } else {
-          const int r = tbl.add_at(cc[k], ww[k], slot);
+          const int r = tbl.template add_at<true>(cc[k], ww[k], slot);
           if (!r) err |= kErrTableFull;
           made = r == 2;
         }
@@ -727,18 +727,17 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
 // evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
 // atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
 // Global tables are packed (key << 32 | sum) with integer weights, split arrays with fp32 ones.
-// Insert half for a global packed table (integer weights): the kBatch entries of a lane first
-// try their home slots with independent CAS operations, all in flight at once (nearly every
-// entry of a long row lands on a community not yet in the table, so the CAS usually creates
-// the key); an entry whose home slot holds its key adds to it, one whose home slot holds
-// another key probes on from there as PackedTable::add does.
+// Insert half for a global packed table (integer weights): a lane's kBatch destinations and
+// their communities are loaded together, then inserted together (PackedTable::add_batch: the
+// slot reads in flight at once, then the CAS operations). A slot is read before any atomic: a
+// CAS tried first adds an atomic for every entry whose community is already in the table, and
+// measured slower on the long rows of R-MAT scale 22.
 __device__ __forceinline__ void insert_scan_global(const Dev& D, const VtxCtx& x, uint32_t v,
                                                    uint32_t e0, uint32_t step, const PackedTable& tbl,
                                                    uint32_t& self_acc, uint32_t& err) {
   const uint32_t* __restrict__ w = reinterpret_cast<const uint32_t*>(D.w);
   for (uint32_t e = e0; e < x.re; e += kBatch * step) {
-    uint32_t uu[kBatch], cc[kBatch], ww[kBatch], hh[kBatch];
-    unsigned long long old[kBatch];
+    uint32_t uu[kBatch], cc[kBatch], ww[kBatch];
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) {
       const uint32_t ek = e + k * step;
@@ -749,25 +748,12 @@ __device__ __forceinline__ void insert_scan_global(const Dev& D, const VtxCtx& x
 #pragma unroll
     for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
 #pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
-      old[k] = kEmptySlot;
-      if (cc[k] != kEmpty && cc[k] != x.cv) {
-        hh[k] = hash_slot(cc[k], tbl.shift);
-        old[k] = atomicCAS(&tbl.slots[hh[k]], kEmptySlot, ((unsigned long long)cc[k] << 32) | ww[k]);
+    for (int k = 0; k < kBatch; ++k)
+      if (cc[k] == x.cv) {
+        self_acc += ww[k];
+        cc[k] = kEmpty;
       }
-    }
-#pragma unroll
-    for (int k = 0; k < kBatch; ++k) {
-      if (cc[k] == kEmpty) continue;
-      if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
-      if (old[k] == kEmptySlot) continue;  // created with its weight
-      if ((uint32_t)(old[k] >> 32) == cc[k]) {
-        atomicAdd(&tbl.slots[hh[k]], (unsigned long long)ww[k]);
-        continue;
-      }
-      const PackedTable rest{tbl.slots, tbl.mask, tbl.shift};
-      if (!rest.add_from((hh[k] + 1) & tbl.mask, cc[k], ww[k])) err |= kErrTableFull;
-    }
+    if (!tbl.add_batch<kBatch>(cc, ww)) err |= kErrTableFull;
   }
 }
 
@@ -1936,14 +1922,13 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
     const uint32_t re = min(D.row[v + 1], rs + kHubInsPiece);
     Acc self_acc = Acc(0);
     if constexpr (WINT) {
-      // kBatch entries per thread: their destinations, communities and home-slot CAS
-      // operations are each issued together; a home slot holding the key is added to, one
-      // holding another key is probed on from (PackedTable::add_from)
+      // kBatch entries per thread: their destinations and communities are loaded together and
+      // inserted together (PackedTable::add_batch), each insert reading its slot before any
+      // atomic: the rows of a large community meet the same neighbouring communities often
       const PackedTable tbl{reinterpret_cast<unsigned long long*>(D.arena_vals) + off, cap - 1u,
                             32u - log2_pow2(cap)};
       for (uint32_t e = rs + threadIdx.x; e < re; e += kBatch * blockDim.x) {
-        uint32_t dd[kBatch], ww[kBatch], hh[kBatch];
-        unsigned long long old[kBatch];
+        uint32_t dd[kBatch], ww[kBatch];
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) {
           const uint32_t ek = e + k * blockDim.x;
@@ -1953,24 +1938,12 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) dd[k] = dd[k] != kEmpty ? D.new_comm[dd[k]] : kEmpty;
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          old[k] = kEmptySlot;
-          if (dd[k] != kEmpty && dd[k] != s) {
-            hh[k] = hash_slot(dd[k], tbl.shift);
-            old[k] = atomicCAS(&tbl.slots[hh[k]], kEmptySlot, ((unsigned long long)dd[k] << 32) | ww[k]);
+        for (int k = 0; k < kBatch; ++k)
+          if (dd[k] == s) {
+            self_acc += (Acc)ww[k];
+            dd[k] = kEmpty;
           }
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          if (dd[k] == kEmpty) continue;
-          if (dd[k] == s) { self_acc += (Acc)ww[k]; continue; }
-          if (old[k] == kEmptySlot) continue;
-          if ((uint32_t)(old[k] >> 32) == dd[k]) {
-            atomicAdd(&tbl.slots[hh[k]], (unsigned long long)ww[k]);
-          } else if (!tbl.add_from((hh[k] + 1) & tbl.mask, dd[k], ww[k])) {
-            err |= kErrTableFull;
-          }
-        }
+        if (!tbl.add_batch<kBatch>(dd, ww)) err |= kErrTableFull;
       }
     } else {
       for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
