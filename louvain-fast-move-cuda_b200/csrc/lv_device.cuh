@@ -87,6 +87,7 @@ struct Ctrl {
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
   uint32_t unit_w;             // integer mode, level 0: every weight is 1, so no kernel loads w
+  uint32_t cluster_on;         // k_opt_cluster runs in table passes (integer weights)
   uint32_t bin_count[kNumBins];
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
@@ -314,38 +315,6 @@ struct PackedTable {
   uint32_t mask, shift;
   __device__ __forceinline__ bool add(uint32_t c, uint32_t w) const {
     return add_from(hash_slot(c, shift), c, w);
-  }
-  // NB inserts at once (entries with c[k] == kEmpty are skipped), each as add() does -- read
-  // the slot, CAS only an empty one, add to the own key, probe on past another key -- but with
-  // the NB home-slot reads issued together, then the NB CAS operations together, so that a
-  // lane waits for two memory round trips per batch instead of two per entry. Adds to an
-  // existing key do not wait for their result. Returns false if some entry found no slot.
-  template <int NB>
-  __device__ __forceinline__ bool add_batch(const uint32_t (&c)[NB], const uint32_t (&w)[NB]) const {
-    uint32_t h[NB];
-    unsigned long long cur[NB];
-#pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      h[k] = hash_slot(c[k], shift);
-      cur[k] = c[k] != kEmpty ? ((volatile unsigned long long*)slots)[h[k]] : 0ull;
-    }
-    bool made[NB];
-#pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      made[k] = false;
-      if (c[k] != kEmpty && cur[k] == kEmptySlot) {
-        cur[k] = atomicCAS(&slots[h[k]], kEmptySlot, ((unsigned long long)c[k] << 32) | w[k]);
-        made[k] = cur[k] == kEmptySlot;  // else cur holds what another insert put there
-      }
-    }
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      if (c[k] == kEmpty || made[k]) continue;
-      if ((uint32_t)(cur[k] >> 32) == c[k]) atomicAdd(&slots[h[k]], (unsigned long long)w[k]);
-      else ok &= add_from((h[k] + 1) & mask, c[k], w[k]);
-    }
-    return ok;
   }
   // add() with the probe sequence starting at slot h (the home slot, or one past it)
   __device__ __forceinline__ bool add_from(uint32_t h, uint32_t c, uint32_t w) const {
