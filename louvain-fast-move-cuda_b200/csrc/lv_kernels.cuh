@@ -878,7 +878,6 @@ __global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterN
     __shared__ uint32_t cself[2];  // CTA 0's: the own-community weight of the current vertex
     __shared__ unsigned long long red[kClusterNT / 32];
     __shared__ uint32_t self_sh;
-    constexpr uint32_t kMask = kClusterSlots - 1u;
     const uint32_t count = C->bin_count[kNumBins - 1];
     const uint32_t* list = D.bins[kNumBins - 1];
     const bool lowest = C->rule_sort != 0;
@@ -896,6 +895,12 @@ __global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterN
       const uint32_t v = list[pos];
       const VtxCtx x = load_vtx(D, v, unit);
       if (!cluster_row(C, x.re - x.rs, x.ng)) continue;  // (cluster-uniform)
+      // the vertex's table: table_cap slots over the 8 parts, so each CTA's part holds
+      // psz = table_cap / 8 slots (a power of two, at most kClusterSlots / 2) and its evaluation
+      // reads only those
+      const uint32_t psz = table_cap(x.re - x.rs, x.ng) / kClusterCTAs < 32u
+                               ? 32u : table_cap(x.re - x.rs, x.ng) / kClusterCTAs;
+      const uint32_t pmask = psz - 1u, pbits = 31u - __clz(psz);
       // inserts: the cluster's threads take the row's entries in turn, kBatch at a time
       uint32_t self_acc = 0;
       const uint32_t step = (uint32_t)kClusterCTAs * kClusterNT;
@@ -916,8 +921,8 @@ __global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterN
           if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
           const uint32_t h = cc[k] * 2654435761u;
           const uint32_t owner = h >> 29;                 // top 3 bits: the CTA (8 per cluster)
-          const uint32_t slot = (h << 3) >> 18;           // next 14 bits: the slot in its part
-          const PackedTable part{cluster.map_shared_rank(tab, owner), kMask, 0u};
+          const uint32_t slot = (h << 3) >> (32u - pbits);  // next bits: the slot in its part
+          const PackedTable part{cluster.map_shared_rank(tab, owner), pmask, 0u};
           if (!part.add_from(slot, cc[k], ww[k])) err |= kErrTableFull;
         }
       }
@@ -929,7 +934,7 @@ __global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterN
       const float self_v = __uint2float_rn(self_sh);
       // evaluation of this CTA's part: every occupied slot, kBatch per thread at a time
       unsigned long long best = 0;
-      for (uint32_t s0 = threadIdx.x; s0 < kClusterSlots; s0 += kBatch * kClusterNT) {
+      for (uint32_t s0 = threadIdx.x; s0 < psz; s0 += kBatch * kClusterNT) {
         uint32_t ck[kBatch], sv[kBatch];
         double ac[kBatch];
 #pragma unroll
@@ -937,7 +942,7 @@ __global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterN
           const uint32_t sl = s0 + k * kClusterNT;
           ck[k] = kEmpty;
           sv[k] = 0;
-          if (sl < kClusterSlots) {
+          if (sl < psz) {
             const unsigned long long xs = tab[sl];
             ck[k] = (uint32_t)(xs >> 32);
             sv[k] = (uint32_t)xs;
