@@ -87,7 +87,6 @@ struct Ctrl {
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
   uint32_t unit_w;             // integer mode, level 0: every weight is 1, so no kernel loads w
-  uint32_t cluster_on;         // k_opt_cluster runs in table passes (integer weights)
   uint32_t bin_count[kNumBins];
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)

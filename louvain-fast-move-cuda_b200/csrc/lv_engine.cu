@@ -31,7 +31,7 @@ namespace lv {
 // Everything that fixes the kernel sequence of a captured run apart from the data: when two
 // runs agree on it, the second reuses the first one's instantiated graph.
 struct GraphKey {
-  int32_t wint, single, mode, fast_first, max_levels, sms, grid_n, grid_sq, grid_block, cluster_grid;
+  int32_t wint, single, mode, fast_first, max_levels, sms, grid_n, grid_sq, grid_block;
   int64_t chunk_edges;
   uint32_t maxdeg[kNumBins], block_cap, team_cap[6];
   int32_t grid_team[6];
@@ -229,33 +229,6 @@ static int occupancy(int device, const void* fn, int block, size_t smem) {
   return occ;
 }
 
-// CTAs for k_opt_cluster: as many whole clusters as can be resident at once (0 if a cluster
-// with its 128 KB of shared memory per CTA cannot be placed on this device). Cached per device.
-static int cluster_blocks(int device, const void* fn) {
-  static std::mutex mu;
-  static std::map<std::pair<int, const void*>, int> cache;
-  std::lock_guard<std::mutex> lk(mu);
-  auto it = cache.find({device, fn});
-  if (it != cache.end()) return it->second;
-  const size_t smem = (size_t)kClusterSlots * 8;
-  int n = 0;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(kClusterCTAs * 64);
-    lc.blockDim = dim3(kClusterNT);
-    lc.dynamicSmemBytes = smem;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, fn, &lc) == cudaSuccess) n = clusters * kClusterCTAs;
-  }
-  cudaGetLastError();
-  cache.emplace(std::make_pair(device, fn), n);
-  return n;
-}
-
-struct HostCtrlSnap {
-  uint32_t it, n, E, n0, G, n_iterating, err, fast, rule_sort;
-};
-
 class Run {
  public:
   lv_context* ctx;
@@ -272,7 +245,6 @@ class Run {
   int grid_sq = 0;          // blocks of k_commit_sq (partials)
   int grid_team[6] = {0};
   int grid_block[2] = {0};
-  int cluster_grid = 0;     // CTAs of k_opt_cluster (0: the cluster path is off)
   uint32_t team_cap[6] = {0};
   uint32_t block_cap = 0;
   cudaStream_t st;
@@ -402,7 +374,6 @@ class Run {
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, (size_t)block_cap * con_slot_bytes());
     grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI>, 512, bsmem));
-    cluster_grid = WI ? cluster_blocks(ctx->device, (const void*)k_opt_cluster<WI>) : 0;
   }
 
   // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
@@ -627,7 +598,6 @@ class Run {
     hc.max_iterations = (uint32_t)std::max(0, cfg.max_iterations);
     hc.threshold = cfg.threshold;
     hc.unit_w = wint ? 1u : 0u;  // k_prep clears it at the first weight other than 1
-    hc.cluster_on = wint && cluster_grid > 0 ? 1u : 0u;
     LV_CUDA(cudaMemcpyAsync(D.ctrl, &hc, offsetof(Ctrl, trace), cudaMemcpyHostToDevice, st));
     std::vector<GraphState> hs(G);
     for (uint32_t g = 0; g < G; ++g) {
@@ -737,10 +707,6 @@ class Run {
     k_opt_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
     k_opt_hub_prep<WI><<<ctx->sms * 4, 256, 0, st>>>(Dd);
-    if (cluster_grid > 0) {
-      k_opt_cluster<WI><<<cluster_grid, kClusterNT, (size_t)kClusterSlots * 8, st>>>(Dd);
-      ++launches;
-    }
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_eval<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     k_opt_hub_decide<<<ctx->sms, 256, 0, st>>>(Dd);
@@ -995,7 +961,6 @@ class Run {
     k.grid_n = grid_n;
     k.grid_sq = grid_sq;
     k.grid_block = grid_block[0];
-    k.cluster_grid = cluster_grid;
     k.chunk_edges = single() ? cfg.chunk_edges : 0;
     for (int b = 0; b < kNumBins; ++b) k.maxdeg[b] = bins.maxdeg[b];
     k.block_cap = bins.block_cap;

@@ -11,13 +11,9 @@
 // not depend on the level and the sequence can be captured once and replayed.
 #pragma once
 
-#include <cooperative_groups.h>
-
 #include "lv_device.cuh"
 
 namespace lv {
-
-namespace cg = cooperative_groups;
 
 // Everything a kernel needs about the current level. Pointers never change during a run
 // (aggregation copies the next level into the same buffers), so a captured launch stays
@@ -153,14 +149,25 @@ __global__ void k_chunk_flags(int dslot) {
   if (blockIdx.x == 0 && threadIdx.x == 0) C->t_pass0 = global_ns();  // first kernel of a pass
   if (!C->chunk_on || !(C->fast || C->rule_sort)) return;
   const uint32_t n = C->n, it = C->it, nch = C->n_chunks;
+  // chunks seen by this thread (the first 32 as bits; later ones, rare, flagged at once),
+  // merged over the warp, so that a flag takes one atomic per warp instead of a read per vertex
+  uint32_t seen = 0;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     if (D.active_it[v] != it) continue;
     const uint32_t d = D.row[v + 1] - D.row[v];
     if (!has_nonloop(D, v, d)) continue;
     uint32_t ch = 0;
     while (ch + 1 < nch && C->chunk_lo[ch + 1] <= v) ++ch;
-    if (!((volatile uint32_t*)C->chunk_any)[ch]) atomicOr(&C->chunk_any[ch], 1u);
+    if (ch < 32) seen |= 1u << ch;
+    else if (!((volatile uint32_t*)C->chunk_any)[ch]) atomicOr(&C->chunk_any[ch], 1u);
   }
+  seen = __reduce_or_sync(kFull, seen);
+  if ((threadIdx.x & 31) == 0)
+    while (seen) {
+      const uint32_t ch = __ffs(seen) - 1;
+      seen &= seen - 1u;
+      if (!((volatile uint32_t*)C->chunk_any)[ch]) atomicOr(&C->chunk_any[ch], 1u);
+    }
 }
 
 // ---- pass: degree binning of the active vertices ----------------------------------------------
@@ -731,17 +738,6 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
 // evaluated chunk by chunk by separate blocks, and the per-vertex argmax key is merged with
 // atomicMax (map[] holds it during a pass; the own-community weight goes to hubself[]).
 // Global tables are packed (key << 32 | sum) with integer weights, split arrays with fp32 ones.
-// Rows of the global-table bin whose table fits a thread-block cluster's shared memory are
-// handled by k_opt_cluster instead (integer weights, table passes, when the host enabled it in
-// Ctrl::cluster_on); the multi-block kernels below skip them.
-constexpr int kClusterCTAs = 8;           // CTAs per cluster (the portable maximum)
-constexpr uint32_t kClusterSlots = 16384;  // packed slots per CTA: 128 KB of shared memory
-constexpr int kClusterNT = 512;
-__device__ __forceinline__ bool cluster_row(const Ctrl* C, uint32_t d, uint32_t ng) {
-  // at most a quarter of the cluster's slots hold keys (distinct keys <= table_cap / 2)
-  return C->cluster_on && table_cap(d, ng) <= (uint32_t)kClusterCTAs * kClusterSlots / 2;
-}
-
 template <bool WINT>
 __device__ __forceinline__ void arena_clear_slot(const Dev& D, uint32_t s) {
   unsigned long long* vals = reinterpret_cast<unsigned long long*>(D.arena_vals);
@@ -792,7 +788,7 @@ __global__ void __launch_bounds__(256) k_opt_hub_scan(int dslot) {
       unsigned long long best = fast_scan<WINT>(D, x, v, pstart + threadIdx.x, blockDim.x);
       best = block_max<256>(best, red);
       if (threadIdx.x == 0 && best) atomicMax(&D.map[pos], best);
-    } else if (!(WINT && cluster_row(C, d, x.ng))) {
+    } else {
       const uint32_t cap = hub_table_cap(d, x.ng);
       const uint32_t off = D.hub_off[pos];
       const bool ok = (unsigned long long)off + cap <= C->arena_slots;
@@ -834,7 +830,6 @@ __global__ void __launch_bounds__(256) k_opt_hub_eval(int dslot) {
     const uint32_t pos = D.hub_owner[c];
     const uint32_t v = D.bins[kNumBins - 1][pos];
     const VtxCtx x = load_vtx(D, v);
-    if (WINT && cluster_row(C, x.re - x.rs, x.ng)) continue;  // (block-uniform) k_opt_cluster's row
     const unsigned long long hs = D.hubself[pos];
     float self_v;
     if (WINT) self_v = Tr::to_float((Acc)hs);
@@ -851,131 +846,6 @@ __global__ void __launch_bounds__(256) k_opt_hub_eval(int dslot) {
     }
     best = block_max<256>(best, red);
     if (threadIdx.x == 0 && best) atomicMax(&D.map[pos], best);
-  }
-}
-
-// Table passes, integer weights: one thread-block cluster per long row (bin 7) whose table
-// fits the cluster. The vertex's community table is spread over the shared memory of the
-// cluster's CTAs (distributed shared memory): a community's hash picks the CTA and the slot in
-// it, and every CTA inserts into every other CTA's part with atomics on the cluster's shared
-// memory, so the table stays on chip -- the multi-block path keeps it in a global arena, whose
-// tables outgrow the L2 cache on large graphs. After a cluster barrier each CTA evaluates the
-// communities in its own part (and empties those slots), the best key goes to map[pos] as in
-// k_opt_hub_eval, and k_opt_hub_decide makes the move. The own community's weight is summed in
-// CTA 0's shared memory (double-buffered by vertex parity, so one barrier pair per vertex
-// suffices). Every CTA of a cluster walks the same vertices, so all reach every barrier.
-template <bool WINT>
-__global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterNT, 1)
-    k_opt_cluster(int dslot) {
-  if constexpr (WINT) {
-    const Dev& D = c_dev[dslot];
-    Ctrl* C = D.ctrl;
-    if (C->fast || !C->cluster_on) return;  // (grid-uniform: no CTA reaches a barrier)
-    cg::cluster_group cluster = cg::this_cluster();
-    const uint32_t rank = cluster.block_rank();
-    extern __shared__ __align__(16) unsigned char smem[];
-    unsigned long long* tab = reinterpret_cast<unsigned long long*>(smem);
-    __shared__ uint32_t cself[2];  // CTA 0's: the own-community weight of the current vertex
-    __shared__ unsigned long long red[kClusterNT / 32];
-    __shared__ uint32_t self_sh;
-    const uint32_t count = C->bin_count[kNumBins - 1];
-    const uint32_t* list = D.bins[kNumBins - 1];
-    const bool lowest = C->rule_sort != 0;
-    const bool unit = unit_weights<WINT>(C);
-    const uint32_t* __restrict__ w = reinterpret_cast<const uint32_t*>(D.w);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t err = 0;
-    for (uint32_t s = threadIdx.x; s < kClusterSlots; s += kClusterNT) tab[s] = kEmptySlot;
-    if (threadIdx.x < 2) cself[threadIdx.x] = 0u;
-    cluster.sync();  // every part is empty before any CTA inserts into it
-    uint32_t* cself0 = cluster.map_shared_rank(cself, 0);
-    const uint32_t ncl = gridDim.x / kClusterCTAs, cid = blockIdx.x / kClusterCTAs;
-    int par = 0;
-    for (uint32_t pos = cid; pos < count; pos += ncl) {
-      const uint32_t v = list[pos];
-      const VtxCtx x = load_vtx(D, v, unit);
-      if (!cluster_row(C, x.re - x.rs, x.ng)) continue;  // (cluster-uniform)
-      // the vertex's table: table_cap slots over the 8 parts, so each CTA's part holds
-      // psz = table_cap / 8 slots (a power of two, at most kClusterSlots / 2) and its evaluation
-      // reads only those
-      const uint32_t psz = table_cap(x.re - x.rs, x.ng) / kClusterCTAs < 32u
-                               ? 32u : table_cap(x.re - x.rs, x.ng) / kClusterCTAs;
-      const uint32_t pmask = psz - 1u, pbits = 31u - __clz(psz);
-      // inserts: the cluster's threads take the row's entries in turn, kBatch at a time
-      uint32_t self_acc = 0;
-      const uint32_t step = (uint32_t)kClusterCTAs * kClusterNT;
-      for (uint32_t e = x.rs + rank * kClusterNT + threadIdx.x; e < x.re; e += kBatch * step) {
-        uint32_t uu[kBatch], cc[kBatch], ww[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          const uint32_t ek = e + k * step;
-          const bool in = ek < x.re;
-          uu[k] = in ? D.col[ek] : v;
-          ww[k] = in ? (unit ? 1u : w[ek]) : 0u;
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          if (cc[k] == kEmpty) continue;
-          if (cc[k] == x.cv) { self_acc += ww[k]; continue; }
-          const uint32_t h = cc[k] * 2654435761u;
-          const uint32_t owner = h >> 29;                 // top 3 bits: the CTA (8 per cluster)
-          const uint32_t slot = (h << 3) >> (32u - pbits);  // next bits: the slot in its part
-          const PackedTable part{cluster.map_shared_rank(tab, owner), pmask, 0u};
-          if (!part.add_from(slot, cc[k], ww[k])) err |= kErrTableFull;
-        }
-      }
-      self_acc = warp_sum(self_acc);
-      if (lane == 0 && self_acc) atomicAdd(&cself0[par], self_acc);
-      cluster.sync();  // the table and the own-community weight are complete
-      if (threadIdx.x == 0) self_sh = cself0[par];
-      __syncthreads();
-      const float self_v = __uint2float_rn(self_sh);
-      // evaluation of this CTA's part: every occupied slot, kBatch per thread at a time
-      unsigned long long best = 0;
-      for (uint32_t s0 = threadIdx.x; s0 < psz; s0 += kBatch * kClusterNT) {
-        uint32_t ck[kBatch], sv[kBatch];
-        double ac[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          const uint32_t sl = s0 + k * kClusterNT;
-          ck[k] = kEmpty;
-          sv[k] = 0;
-          if (sl < psz) {
-            const unsigned long long xs = tab[sl];
-            ck[k] = (uint32_t)(xs >> 32);
-            sv[k] = (uint32_t)xs;
-            if (ck[k] != kEmpty) tab[sl] = kEmptySlot;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) ac[k] = ck[k] != kEmpty ? D.a[ck[k]] : 0.0;
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-          if (ck[k] == kEmpty) continue;
-          const float diff = __fsub_rn(__uint2float_rn(sv[k]), self_v);
-          const double p = gain_p(x.kv, x.own_minus_k, ac[k]);
-          const float g = gain_fast(diff, p, x.inv_m, x.inv_2m2, x.m, x.two_m2);
-          if (g > 0.0f) {
-            const unsigned long long key = argmax_key(g, ck[k], lowest);
-            if (key > best) best = key;
-          }
-        }
-      }
-      best = team_max<32>(best, kFull);
-      if (lane == 0) red[wid] = best;
-      __syncthreads();
-      if (wid == 0) {
-        unsigned long long y = lane < kClusterNT / 32 ? red[lane] : 0ull;
-        y = team_max<32>(y, kFull);
-        if (lane == 0 && y) atomicMax(&D.map[pos], y);
-      }
-      if (rank == 0 && threadIdx.x == 0) cself[par ^ 1] = 0u;  // the next vertex's sum
-      cluster.sync();  // every part evaluated and empty again; red and self_sh free
-      par ^= 1;
-    }
-    if (err) report_err(C, err, 9);  // k_opt_cluster
   }
 }
 
