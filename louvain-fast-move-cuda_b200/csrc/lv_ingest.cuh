@@ -171,13 +171,28 @@ __global__ void __launch_bounds__(kIScanNT) k_iscan_apply(const uint32_t* in, ui
 
 // ---- rows ----------------------------------------------------------------------------------
 // Entries per row: each pair puts one entry into the row of each end (ids relative to the
-// minimum); a row with no entry means a missing id.
+// minimum); a row with no entry means a missing id. Lanes of a warp that add to the same row
+// (hub rows of a skewed graph are hit often) combine their counts into one atomic.
+__device__ __forceinline__ void warp_add_row(uint32_t* cnt, uint32_t r) {
+  const unsigned m = __match_any_sync(__activemask(), r);
+  if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt[r], (uint32_t)__popc(m));
+}
+// The position of this lane's entry in row r: one atomic per group of lanes writing row r.
+__device__ __forceinline__ uint32_t warp_claim_row(uint32_t* cursor, uint32_t r) {
+  const unsigned m = __match_any_sync(__activemask(), r);
+  const int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&cursor[r], (uint32_t)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + __popc(m & lanemask_lt());
+}
+
 __global__ void k_pair_count(const int32_t* val, uint64_t npairs, int mn, uint32_t* cnt) {
   for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
        p += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t a = (uint32_t)((long long)val[2 * p] - mn), b = (uint32_t)((long long)val[2 * p + 1] - mn);
-    atomicAdd(&cnt[a], 1u);
-    atomicAdd(&cnt[b], 1u);
+    warp_add_row(cnt, a);
+    warp_add_row(cnt, b);
   }
 }
 
@@ -194,8 +209,8 @@ __global__ void k_pair_scatter(const int32_t* val, uint64_t npairs, int mn, uint
   for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
        p += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t a = (uint32_t)((long long)val[2 * p] - mn), b = (uint32_t)((long long)val[2 * p + 1] - mn);
-    buf[atomicAdd(&cursor[a], 1u)] = b;
-    buf[atomicAdd(&cursor[b], 1u)] = a;
+    buf[warp_claim_row(cursor, a)] = b;
+    buf[warp_claim_row(cursor, b)] = a;
   }
 }
 
