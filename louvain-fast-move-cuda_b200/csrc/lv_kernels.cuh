@@ -2275,9 +2275,10 @@ __global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint
 
 // Copy the gapped contracted rows into the dense next-level CSR (col/w), move k' and gid'.
 // The output is cut into chunks of kCompactChunk entries, one block per chunk, so a row of any
-// length is copied by as many blocks as it spans; each block stages the offsets of the rows
-// that overlap its chunk (dense start and gapped source start) in shared memory, and its warps
-// take those rows in turn, the lanes of a warp copying consecutive entries of one row.
+// length is copied by as many blocks as it spans; each block stages the offsets (dense and
+// gapped) of the rows that overlap its chunk in shared memory and finds every entry's row by
+// binary search there. (Warps taking whole rows instead measured 2.8x slower: most contracted
+// rows are short.)
 constexpr uint32_t kCompactChunk = 2048;
 
 template <bool WINT>
@@ -2291,7 +2292,6 @@ __global__ void __launch_bounds__(256) k_agg_compact(int dslot) {
   const uint32_t E2 = D.rowB[n2];
   const Wt* __restrict__ win = reinterpret_cast<const Wt*>(D.wB);
   Wt* __restrict__ wout = reinterpret_cast<Wt*>(D.w);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t nchunks = (E2 + kCompactChunk - 1) / kCompactChunk;
   for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const uint32_t start = ch * kCompactChunk;
@@ -2299,26 +2299,27 @@ __global__ void __launch_bounds__(256) k_agg_compact(int dslot) {
     if (threadIdx.x == 0) {
       uint32_t lo = 0, hi = n2;  // last row with rowB[r] <= start
       while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (D.rowB[mid] <= start) lo = mid; else hi = mid; }
-      uint32_t lo2 = lo;         // last row with rowB[r] < end
+      uint32_t r1 = lo;           // first row with rowB[r] >= end
       hi = n2;
+      uint32_t lo2 = lo;
       while (hi - lo2 > 1) { const uint32_t mid = (lo2 + hi) >> 1; if (D.rowB[mid] < end) lo2 = mid; else hi = mid; }
+      r1 = lo2 + 1;
       r0_sh = lo;
-      nr_sh = lo2 + 1 - lo;  // rows lo..lo2 overlap the chunk (every row has an entry: <= kCompactChunk)
+      nr_sh = r1 - lo;  // rows lo..r1-1 overlap the chunk (every row has an entry: <= kCompactChunk)
     }
     __syncthreads();
     const uint32_t r0 = r0_sh, nr = nr_sh;
     for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) {
       rs[i] = D.rowB[r0 + i];
-      if (i < nr) src0[i] = (uint32_t)D.cd[r0 + i];
+      if (i < nr) src0[i] = (uint32_t)D.cd[r0 + i];  // the row's start in the gapped rows
     }
     __syncthreads();
-    for (uint32_t r = wid; r < nr; r += blockDim.x >> 5) {
-      const uint32_t a = max(rs[r], start), b = min(rs[r + 1], end);
-      const uint32_t so = src0[r] - rs[r];  // source index = dense index + so
-      for (uint32_t p = a + lane; p < b; p += 32) {
-        D.col[p] = D.colB[p + so];
-        wout[p] = win[p + so];
-      }
+    for (uint32_t p = start + threadIdx.x; p < end; p += blockDim.x) {
+      uint32_t lo = 0, hi = nr;  // rs[lo] <= p < rs[lo + 1]
+      while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (rs[mid] <= p) lo = mid; else hi = mid; }
+      const uint32_t src = src0[lo] + (p - rs[lo]);
+      D.col[p] = D.colB[src];
+      wout[p] = win[src];
     }
     __syncthreads();
   }
