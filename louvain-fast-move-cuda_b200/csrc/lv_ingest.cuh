@@ -461,16 +461,42 @@ __global__ void __launch_bounds__(kIngestBlockNT) k_rows_bitmap(const uint32_t* 
   }
 }
 
-// Distinct, sorted rows (at their bucket starts) -> the dense CSR, a warp per row.
-__global__ void k_rows_copy(const uint32_t* start, const uint32_t* ulen, const int64_t* row_ptr, uint32_t range,
-                            const uint32_t* buf, int32_t* col) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = warp; v < range; v += nwarps) {
-    const uint32_t s0 = start[v], len = ulen[v];
-    const int64_t d0 = row_ptr[v];
-    for (uint32_t i = lane; i < len; i += 32) col[d0 + i] = (int32_t)buf[s0 + i];
+// Distinct, sorted rows (at their bucket starts) -> the dense CSR. The output is cut into chunks
+// of kRowsCopyChunk entries, one block per chunk: the block stages the dense and bucket starts
+// of the rows that overlap its chunk and finds each entry's row by binary search there (most
+// rows are short, so a warp per row would leave most lanes idle).
+constexpr uint32_t kRowsCopyChunk = 2048;
+
+__global__ void __launch_bounds__(256) k_rows_copy(const uint32_t* start, const int64_t* row_ptr, uint32_t range,
+                                                   uint64_t ne, const uint32_t* buf, int32_t* col) {
+  __shared__ uint32_t rs[kRowsCopyChunk + 2], src0[kRowsCopyChunk + 1];
+  __shared__ uint32_t r0_sh, nr_sh;
+  const uint64_t nchunks = (ne + kRowsCopyChunk - 1) / kRowsCopyChunk;
+  for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const uint32_t cs = (uint32_t)(ch * kRowsCopyChunk);
+    const uint32_t ce = (uint32_t)min((uint64_t)cs + kRowsCopyChunk, ne);
+    if (threadIdx.x == 0) {
+      uint32_t lo = 0, hi = range;  // last row with row_ptr[r] <= cs
+      while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if ((uint64_t)row_ptr[mid] <= cs) lo = mid; else hi = mid; }
+      uint32_t lo2 = lo;            // last row with row_ptr[r] < ce
+      hi = range;
+      while (hi - lo2 > 1) { const uint32_t mid = (lo2 + hi) >> 1; if ((uint64_t)row_ptr[mid] < ce) lo2 = mid; else hi = mid; }
+      r0_sh = lo;
+      nr_sh = lo2 + 1 - lo;  // every row has an entry, so at most kRowsCopyChunk rows
+    }
+    __syncthreads();
+    const uint32_t r0 = r0_sh, nr = nr_sh;
+    for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) {
+      rs[i] = (uint32_t)row_ptr[r0 + i];
+      if (i < nr) src0[i] = start[r0 + i];
+    }
+    __syncthreads();
+    for (uint32_t p = cs + threadIdx.x; p < ce; p += blockDim.x) {
+      uint32_t lo = 0, hi = nr;  // rs[lo] <= p < rs[lo + 1]
+      while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (rs[mid] <= p) lo = mid; else hi = mid; }
+      col[p] = (int32_t)buf[src0[lo] + (p - rs[lo])];
+    }
+    __syncthreads();
   }
 }
 
@@ -667,7 +693,7 @@ static void ingest_run(lv_context* ctx, const char* text_in, int64_t len, int32_
     cudaGetLastError();
     throw Fail{LV_ERR_NOMEM, "cudaMalloc of the CSR destinations failed"};
   }
-  k_rows_copy<<<grid, 256, 0, st>>>(rstart, ulen, row_ptr, (uint32_t)range, buf, col);
+  k_rows_copy<<<grid, 256, 0, st>>>(rstart, row_ptr, (uint32_t)range, ne, buf, col);
   const cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaFree(row_ptr);
