@@ -16,9 +16,9 @@
 //   rows     : a scan of the counts places the rows; every pair writes each end into the
 //              other's row (a self-loop pair writes its id twice into its own row)
 //   CSR      : each row sorted and deduplicated on its own -- a warp bitonic sort in registers
-//              for rows of up to 32 entries (one per lane) and up to 256 (eight per lane), a
-//              block bitonic sort in shared memory up to kIngestBlockRow, and above that a
-//              bitmap of the row's id range in global memory
+//              for rows of up to 32 entries (one per lane), 256 (eight per lane) and 1024 (32
+//              per lane), a block bitonic sort in shared memory up to kIngestBlockRow, and above
+//              that a bitmap of the row's id range in global memory
 //              whose set bits read out in order are the sorted distinct ids; a row keeps its
 //              own id twice when the graph has that self-loop pair (graph.cu:68-79 emits both
 //              directions of it); a second scan of the row lengths gives the row offsets
@@ -217,53 +217,60 @@ __global__ void k_pair_scatter(const int32_t* val, uint64_t npairs, int mn, uint
 
 constexpr uint32_t kIngestWarpRow = 32;     // rows sorted by one warp, one entry per lane
 constexpr uint32_t kIngestWarp8Row = 256;   // rows sorted by one warp, eight entries per lane
+constexpr uint32_t kIngestWarp32Row = 1024; // rows sorted by one warp, 32 entries per lane
 constexpr uint32_t kIngestBlockRow = 4096;  // rows sorted by one block in shared memory
 constexpr int kIngestBlockNT = 512;
 
-// Rows longer than a warp's: appended to the eight-per-lane list (counts[2]), the block list
-// (counts[0]) or the bitmap list (counts[1]).
+// Rows longer than a warp's: appended to the block list (counts[0]), the bitmap list
+// (counts[1]), the eight-per-lane list (counts[2]) or the 32-per-lane list (counts[3]).
 __global__ void k_rows_classify(const uint32_t* cnt, uint32_t range, uint32_t* mid, uint32_t* big,
-                                uint32_t* mid8, uint32_t* counts) {
+                                uint32_t* mid8, uint32_t* mid32, uint32_t* counts) {
   for (uint32_t base = blockIdx.x * blockDim.x; base < range; base += gridDim.x * blockDim.x) {
     const uint32_t v = base + threadIdx.x;
     const uint32_t c = v < range ? cnt[v] : 0u;
-    const int cls = c > kIngestBlockRow ? 1 : (c > kIngestWarp8Row ? 0 : (c > kIngestWarpRow ? 2 : -1));
-    const uint32_t pm = warp_append(cls, 0, &counts[0]);
-    if (pm != kEmpty) mid[pm] = v;
-    const uint32_t pb = warp_append(cls, 1, &counts[1]);
-    if (pb != kEmpty) big[pb] = v;
-    const uint32_t p8 = warp_append(cls, 2, &counts[2]);
-    if (p8 != kEmpty) mid8[p8] = v;
+    const int cls = c > kIngestBlockRow ? 1
+                    : c > kIngestWarp32Row ? 0
+                    : c > kIngestWarp8Row ? 3
+                    : c > kIngestWarpRow ? 2 : -1;
+    uint32_t* lists[4] = {mid, big, mid8, mid32};
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const uint32_t pos = warp_append(cls, b, &counts[b]);
+      if (pos != kEmpty) lists[b][pos] = v;
+    }
   }
 }
 
-// Rows of 33..256 entries, one warp each: the row padded to 256 held as eight registers per lane
-// (element q * 32 + lane in register q), sorted by a bitonic network whose partners at distance
-// 32 and more sit in the lane's own registers and below 32 in another lane's (shuffles); then
-// the distinct ids in order, the row's own id twice, back at the row's start.
-__global__ void k_rows_warp8(const uint32_t* start, const uint32_t* cnt, const uint32_t* mid8,
-                             const uint32_t* counts, uint32_t* buf, uint32_t* ulen) {
+// Rows of up to 32 * PER entries, one warp each: the row padded to 32 * PER held as PER
+// registers per lane (element q * 32 + lane in register q), sorted by a bitonic network whose
+// partners at distance 32 and more sit in the lane's own registers and below 32 in another
+// lane's (shuffles); then the distinct ids in order, the row's own id twice, back at the row's
+// start. `rows` lists the rows (count *n_rows).
+template <int PER>
+__global__ void k_rows_warpn(const uint32_t* start, const uint32_t* cnt, const uint32_t* rows,
+                             const uint32_t* n_rows, uint32_t* buf, uint32_t* ulen) {
+  constexpr int P = 32 * PER;
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t n8 = counts[2];
-  for (uint32_t r = warp; r < n8; r += nwarps) {
-    const uint32_t v = mid8[r];
+  const uint32_t nr = *n_rows;
+  for (uint32_t r = warp; r < nr; r += nwarps) {
+    const uint32_t v = rows[r];
     const uint32_t c = cnt[v], s0 = start[v];
-    uint32_t x[8];
+    uint32_t x[PER];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < PER; ++q) {
       const uint32_t i = (uint32_t)q * 32u + lane;
       x[q] = i < c ? buf[s0 + i] : kEmpty;
     }
 #pragma unroll
-    for (int k = 2; k <= 256; k <<= 1) {
+    for (int k = 2; k <= P; k <<= 1) {
 #pragma unroll
       for (int j = k >> 1; j > 0; j >>= 1) {
         if (j >= 32) {
           const int jq = j >> 5;
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
+          for (int q = 0; q < PER; ++q) {
             if (q & jq) continue;
             const int q2 = q | jq;
             const bool up = ((q * 32 + lane) & k) == 0;
@@ -272,7 +279,7 @@ __global__ void k_rows_warp8(const uint32_t* start, const uint32_t* cnt, const u
           }
         } else {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
+          for (int q = 0; q < PER; ++q) {
             const uint32_t y = __shfl_xor_sync(kFull, x[q], j);
             const bool up = ((q * 32 + lane) & k) == 0, low = (lane & j) == 0;
             x[q] = (low == up) ? min(x[q], y) : max(x[q], y);
@@ -282,10 +289,10 @@ __global__ void k_rows_warp8(const uint32_t* start, const uint32_t* cnt, const u
     }
     // distinct ids in element order: the previous element of q*32+lane is lane-1 in register q,
     // or for lane 0 lane 31 in register q-1
-    uint32_t emit[8], off[8];
+    uint32_t emit[PER], off[PER];
     uint32_t run = 0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < PER; ++q) {
       const uint32_t up1 = __shfl_up_sync(kFull, x[q], 1);
       const uint32_t last_prev = q > 0 ? __shfl_sync(kFull, x[q > 0 ? q - 1 : 0], 31) : kEmpty;
       const uint32_t prev = lane > 0 ? up1 : last_prev;
@@ -298,7 +305,7 @@ __global__ void k_rows_warp8(const uint32_t* start, const uint32_t* cnt, const u
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+    for (int q = 0; q < PER; ++q)
       for (uint32_t t = 0; t < emit[q]; ++t) buf[s0 + off[q] + t] = x[q];
     if (lane == 0) ulen[v] = run;
   }
@@ -336,7 +343,7 @@ __global__ void k_rows_warp(const uint32_t* start, const uint32_t* cnt, uint32_t
   }
 }
 
-// Rows of 33..kIngestBlockRow entries, one block each: bitonic sort in shared memory.
+// Rows of 1025..kIngestBlockRow entries, one block each: bitonic sort in shared memory.
 __global__ void __launch_bounds__(kIngestBlockNT) k_rows_block(const uint32_t* start, const uint32_t* cnt,
                                                                const uint32_t* mid, const uint32_t* counts,
                                                                uint32_t* buf, uint32_t* ulen) {
@@ -650,19 +657,21 @@ static void ingest_run(lv_context* ctx, const char* text_in, int64_t len, int32_
   k_pair_scatter<<<grid, 256, 0, st>>>(val, npairs, hmm[0], cursor, buf);
   bval.reset();
   // each row sorted and deduplicated in place: warp, block or bitmap by its length
-  DevBuf bmid, bbig, bmid8, bcls, bulen;
+  DevBuf bmid, bbig, bmid8, bmid32, bcls, bulen;
   uint32_t* mid = bmid.alloc<uint32_t>(range);
   uint32_t* big = bbig.alloc<uint32_t>(range);
   uint32_t* mid8 = bmid8.alloc<uint32_t>(range);
-  uint32_t* cls = bcls.alloc<uint32_t>(3);
-  LV_CUDA(cudaMemsetAsync(cls, 0, 12, st));
-  k_rows_classify<<<grid, 256, 0, st>>>(cntr, (uint32_t)range, mid, big, mid8, cls);
-  uint32_t hcls[3] = {0, 0, 0};
-  LV_CUDA(cudaMemcpyAsync(hcls, cls, 12, cudaMemcpyDeviceToHost, st));
+  uint32_t* mid32 = bmid32.alloc<uint32_t>(range);
+  uint32_t* cls = bcls.alloc<uint32_t>(4);
+  LV_CUDA(cudaMemsetAsync(cls, 0, 16, st));
+  k_rows_classify<<<grid, 256, 0, st>>>(cntr, (uint32_t)range, mid, big, mid8, mid32, cls);
+  uint32_t hcls[4] = {0, 0, 0, 0};
+  LV_CUDA(cudaMemcpyAsync(hcls, cls, 16, cudaMemcpyDeviceToHost, st));
   uint32_t* ulen = bulen.alloc<uint32_t>(range + 1);
   LV_CUDA(cudaMemsetAsync(ulen + range, 0, 4, st));
   k_rows_warp<<<grid, 256, 0, st>>>(rstart, cntr, (uint32_t)range, buf, ulen);
-  k_rows_warp8<<<grid, 256, 0, st>>>(rstart, cntr, mid8, cls, buf, ulen);
+  k_rows_warpn<8><<<grid, 256, 0, st>>>(rstart, cntr, mid8, cls + 2, buf, ulen);
+  k_rows_warpn<32><<<grid, 256, 0, st>>>(rstart, cntr, mid32, cls + 3, buf, ulen);
   k_rows_block<<<ctx->sms * 2, kIngestBlockNT, 0, st>>>(rstart, cntr, mid, cls, buf, ulen);
   LV_CUDA(cudaStreamSynchronize(st));
   DevBuf bbm;

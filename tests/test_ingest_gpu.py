@@ -78,3 +78,40 @@ def test_ingest_errors(lv, engine):
     # the context still works
     g, _ = _check(lv, engine, b"0 1\n1 2\n")
     g.close()
+
+
+def test_ingest_every_row_class(lv, engine):
+    """Rows of every size class the device sort treats differently (one entry per lane, eight
+    and 32 per lane, a block, a bitmap over the row's id range), each with duplicate pairs in
+    both orders and, for some hubs, the hub's own self-loop pair (kept twice in its row)."""
+    rng = np.random.default_rng(7)
+    n = 20000
+    pairs = [np.stack([np.arange(n - 1), np.arange(1, n)], 1)]  # a path keeps the ids contiguous
+    for hub, deg, loop in ((10, 20, False), (11, 200, True), (12, 900, False), (13, 3000, True),
+                           (14, 9000, True), (15, 15000, False)):
+        nb = rng.choice(n, size=deg, replace=False)
+        pairs.append(np.stack([np.full(deg, hub), nb], 1))
+        dup = nb[: deg // 3]
+        pairs.append(np.stack([dup, np.full(dup.size, hub)], 1))  # the same pairs reversed
+        if loop:
+            pairs.append(np.array([[hub, hub], [hub, hub]]))
+    p = np.concatenate(pairs)
+    p = p[rng.permutation(len(p))]
+    text = "\n".join(f"{a} {b}" for a, b in p.tolist()).encode()
+    g, csr = _check(lv, engine, text)
+    deg = np.diff(csr.row_ptr)
+    assert deg.max() > 4096 and ((deg > 1024) & (deg <= 4096)).any() and ((deg > 256) & (deg <= 1024)).any()
+    g.close()
+
+
+def test_ingest_rmat16_raw_pairs(lv, engine, graphs):
+    """Raw R-MAT pairs at scale 16 (1 M pairs with duplicates and self-loops): hub rows far above
+    4,096 entries, as in the benchmark's scale-22 input."""
+    u, v = graphs.rmat_pairs(16, 16, seed=2)
+    ids = np.unique(np.concatenate([u, v]))
+    remap = np.searchsorted(ids, np.concatenate([u, v]))
+    a, b = remap[: u.size], remap[u.size:]
+    text = graphs.edge_list_bytes(a, b)
+    g, csr = _check(lv, engine, text)
+    assert np.diff(csr.row_ptr).max() > 4096
+    g.close()
