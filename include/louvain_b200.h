@@ -161,10 +161,12 @@ lv_status lv_run_batch(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_off
 /* Autotuner (no reference counterpart): times full runs of a sample -- one graph
  * (n_graphs = 1, vtx_offsets = {0, n}) or a packed batch -- under a fixed set of candidate
  * degree-bin tables (the boundaries that pick 4 / 8 / 16 / 32 lanes, a block or many blocks
- * per row, and with them each row's hash-table capacity), `trials` runs each, keeps the
- * fastest. The chosen table becomes the context's cfg.bin_max_degree for later runs and is
- * returned in *out_cfg; *out_ms = its best run time. Results do not depend on the table for
- * integer weights (every table computes the same sums). */
+ * per row, and with them each row's hash-table capacity): per candidate one untimed run
+ * (which captures its level loop), then `trials` timed runs of the level loop alone; the
+ * fastest candidate is kept if it beats the first (built-in) table by more than 3 %, else the
+ * built-in table is kept. The chosen table becomes the context's cfg.bin_max_degree for later
+ * runs and is returned in *out_cfg; *out_ms = its best run time. Results do not depend on the
+ * table for integer weights (every table computes the same sums). */
 lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offsets,
                       const int64_t* row_ptr, const int32_t* col, const float* w, int32_t in_mem,
                       int32_t trials, lv_config* out_cfg, double* out_ms);

@@ -60,12 +60,17 @@ struct GraphState {
 
 // Hash-table capacity for a row of d entries in a graph of ng vertices: twice the number of
 // distinct keys it can hold (at most min(d, ng)), rounded up to a power of two.
+// (2 x the smallest power of two >= k: 2 << ceil(log2 k), from the leading zeros of k - 1;
+// k <= 2^30 since rows hold at most 2^30 entries)
 __host__ __device__ __forceinline__ uint32_t table_cap(uint32_t d, uint32_t ng) {
   uint32_t k = d < ng ? d : ng;
   if (k < 1) k = 1;
-  uint32_t p = 2;
-  while (p < 2u * k) p <<= 1;
-  return p;
+#ifdef __CUDA_ARCH__
+  const int lz = __clz((int)(k - 1u));  // 32 when k == 1
+#else
+  const int lz = k == 1 ? 32 : __builtin_clz(k - 1u);
+#endif
+  return 2u << (32 - lz);
 }
 
 struct TraceRec {

@@ -349,9 +349,10 @@ class Run {
   }
 
   // Shared memory per table slot of the gain and contraction kernels: key + sum, plus half a
-  // u16 of key list per slot (the list holds cap / 2 slot indices).
+  // u16 of key list per slot (the list holds cap / 2 slot indices); the gain kernels with
+  // integer weights also list the communities' totals (cap / 2 u32).
   size_t con_slot_bytes() const { return 4 + acc_size() + 1; }
-  size_t opt_slot_bytes() const { return 4 + acc_size() + 1; }
+  size_t opt_slot_bytes() const { return 4 + acc_size() + 1 + (wint ? 2 : 0); }
 
   template <int T>
   void team_grid(int b, const void* opt_fn, const void* con_fn) {
@@ -532,6 +533,7 @@ class Run {
     D.apply_items = dalloc<unsigned long long>(ctx, owned, (size_t)n + E / kHubPiece + 16, st);
     D.movers = dalloc<uint32_t>(ctx, owned, n, st);
     D.cn = dalloc<unsigned long long>(ctx, owned, n, st);
+    D.ca = dalloc<unsigned long long>(ctx, owned, n, st);
     D.gs = dalloc<GraphState>(ctx, owned, G, st);
     D.ctrl = dalloc<Ctrl>(ctx, owned, 1, st);
     D.partials = dalloc<double>(ctx, owned, kMaxPartials, st);
@@ -697,7 +699,7 @@ class Run {
     const size_t slot = opt_slot_bytes();
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
     k_chunk_flags<<<grid_n, 256, 0, st>>>(Dd);
-    k_bin_vertices<<<grid_n, 256, 0, st>>>(Dd, bins);
+    k_bin_vertices<<<grid_n, 256, 0, st>>>(Dd, bins, WI ? 1 : 0);
     k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(Dd, 0, team_cap[0]);
     k_opt_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
     k_opt_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
@@ -1595,15 +1597,16 @@ lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offs
     if (in_mem == LV_MEM_DEVICE) LV_CUDA(cudaMemcpy(&n, vtx_offsets + n_graphs, 8, cudaMemcpyDeviceToHost));
     else n = vtx_offsets[n_graphs];
     const lv_config base = ctx->cfg;
-    double best_ms = 1e300;
+    double best_ms = 1e300, default_ms = 1e300;
     int best = -1;
     for (int c = 0; c < kTuneN; ++c) {
+      // one untimed run first (it captures and instantiates the candidate's level loop), then
+      // the level loop alone is timed: upload and device graph build do not depend on the bins
       double ms_c = 1e300;
-      for (int t = 0; t < trials; ++t) {
+      for (int t = 0; t <= trials; ++t) {
         lv::Run r(ctx);
         for (int b = 0; b < 7; ++b) r.cfg.bin_max_degree[b] = kTuneCandidates[c][b];
         r.cfg.bin_max_degree[7] = 0;
-        LV_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
         try {
           r.init((uint32_t)n_graphs, n_graphs > 1 ? vtx_offsets : nullptr, n, row_ptr, col, w, in_mem);
         } catch (const lv::Fail& e) {
@@ -1611,17 +1614,26 @@ lv_status lv_autotune(lv_context* ctx, int32_t n_graphs, const int64_t* vtx_offs
           if (e.st != LV_ERR_ARGUMENT || c == 0) throw;
           break;
         }
+        LV_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
         r.louvain();
         LV_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
         LV_CUDA(cudaEventSynchronize(ctx->ev[1]));
         float ms = 0;
         LV_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-        ms_c = std::min(ms_c, (double)ms);
+        if (t > 0) ms_c = std::min(ms_c, (double)ms);
       }
+      if (c == 0) default_ms = ms_c;
       if (ms_c < best_ms) {
         best_ms = ms_c;
         best = c;
       }
+    }
+    // another table replaces the first (built-in) one only when it is clearly faster on the
+    // sample: differences within a few percent are run-to-run noise, and a sample's optimum
+    // carries over to the larger graphs it stands for only when the margin is real
+    if (best != 0 && best_ms > 0.97 * default_ms) {
+      best = 0;
+      best_ms = default_ms;
     }
     ctx->cfg = base;
     for (int b = 0; b < 7; ++b) ctx->cfg.bin_max_degree[b] = kTuneCandidates[best][b];

@@ -57,6 +57,10 @@ struct Dev {
   int32_t* out;              // [n0] final community ids
   unsigned long long* scan_tmp;  // [(n + 1) / kScanTile + 2] tile sums of the scans
   unsigned long long* cn;    // [n] apply phase: (new_comm << 32) | comm, one gather per entry
+  // [n] table passes with integer weights: (total of comm[v] << 32) | comm[v], written by
+  // k_bin_vertices, so that an entry's community and that community's total (a u32: integer
+  // totals stay below 2m < 2^32) arrive with one gather
+  unsigned long long* ca;
   // refinement (allocated only when it is on; lv_refine.cuh)
   uint32_t* ref;             // [n] refined partition
   uint32_t* ref_new;         // [n] its pass targets
@@ -171,60 +175,132 @@ __global__ void k_chunk_flags(int dslot) {
 }
 
 // ---- pass: degree binning of the active vertices ----------------------------------------------
-__global__ void k_bin_vertices(int dslot, BinCfg B) {
+// Blocks take tiles of kBinTile consecutive vertices (kBinPer per thread). A tile's bin sizes
+// are summed over the block first, so that each bin's list space is claimed with one atomic
+// per tile and bin (one per warp and bin contended on the eight counters and made the kernel
+// atomic-bound), and the pass accounting is added once per block.
+constexpr int kBinNT = 256, kBinPer = 4, kBinTile = kBinNT * kBinPer;
+
+__global__ void __launch_bounds__(kBinNT) k_bin_vertices(int dslot, BinCfg B, int pack_ca) {
   const Dev& D = c_dev[dslot];
   Ctrl* C = D.ctrl;
   const uint32_t n = C->n, it = C->it;
+  // table passes with integer weights: every vertex's (total, community) word for the gathers
+  // of the gain kernels (the totals do not change before this pass's apply kernels)
+  if (pack_ca && !C->fast)
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+      const uint32_t c = D.comm[v];
+      D.ca[v] = ((unsigned long long)(uint32_t)D.a[c] << 32) | c;
+    }
   uint32_t v_end = n;
   if (C->chunk_on && (C->fast || C->rule_sort)) {
     for (uint32_t ch = 0; ch < C->n_chunks; ++ch)
       if (!C->chunk_any[ch]) { v_end = C->chunk_lo[ch]; break; }
   }
   const bool want_off = !C->fast;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t v = base + threadIdx.x;
-    int bin = -1;
-    uint32_t d = 0, cap = 0;
-    if (v < v_end && D.active_it[v] == it) {
-      const uint32_t g = D.gid ? D.gid[v] : 0u;
-      if (D.gs[g].phase == kIterating) {
-        d = D.row[v + 1] - D.row[v];
-        if (d > 0) {
-          bin = bin_of(B, d);
-          // a long row whose distinct communities fit the shared table stays in bin 6
-          if (bin == kNumBins - 1) {
-            cap = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
-            if (cap <= B.block_cap) bin = kNumBins - 2;
+  constexpr int NW = kBinNT / 32;
+  __shared__ uint32_t s_cnt[NW][kNumBins];  // per warp and bin: members in this tile, then list base
+  __shared__ unsigned long long s_acc[NW];
+  __shared__ uint32_t s_accv[NW];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t lt = lanemask_lt();
+  unsigned long long act_e = 0;  // pass accounting for the roofline: entries and vertices binned
+  uint32_t act_v = 0;
+  for (uint32_t t0 = blockIdx.x * kBinTile; t0 < n; t0 += gridDim.x * kBinTile) {
+    int bin[kBinPer];
+    uint32_t dd[kBinPer], cap[kBinPer];
+#pragma unroll
+    for (int j = 0; j < kBinPer; ++j) {
+      const uint32_t v = t0 + j * kBinNT + threadIdx.x;
+      bin[j] = -1;
+      dd[j] = 0;
+      cap[j] = 0;
+      if (v < v_end && D.active_it[v] == it) {
+        const uint32_t g = D.gid ? D.gid[v] : 0u;
+        if (D.gs[g].phase == kIterating) {
+          const uint32_t d = D.row[v + 1] - D.row[v];
+          if (d > 0) {
+            int b = bin_of(B, d);
+            // a long row whose distinct communities fit the shared table stays in bin 6
+            if (b == kNumBins - 1) {
+              cap[j] = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
+              if (cap[j] <= B.block_cap) b = kNumBins - 2;
+            }
+            bin[j] = b;
+            dd[j] = d;
+            act_e += d;
+            ++act_v;
           }
         }
       }
     }
+    // members per bin in this warp (lane b keeps bin b's count)
+    uint32_t mine = 0;
 #pragma unroll
     for (int b = 0; b < kNumBins; ++b) {
-      const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
-      if (pos != kEmpty) {
+      uint32_t c = 0;
+#pragma unroll
+      for (int j = 0; j < kBinPer; ++j) c += __popc(__ballot_sync(kFull, bin[j] == b));
+      if (lane == b) mine = c;
+    }
+    if (lane < kNumBins) s_cnt[wid][lane] = mine;
+    __syncthreads();
+    if (threadIdx.x < kNumBins) {
+      // one claim per bin for the whole tile; warps get consecutive ranges in warp order
+      const int b = threadIdx.x;
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) tot += s_cnt[w][b];
+      uint32_t base = tot ? atomicAdd(&C->bin_count[b], tot) : 0u;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const uint32_t c = s_cnt[w][b];
+        s_cnt[w][b] = base;
+        base += c;
+      }
+    }
+    __syncthreads();
+    uint32_t run = lane < kNumBins ? s_cnt[wid][lane] : 0u;  // lane b: next position in bin b
+#pragma unroll
+    for (int j = 0; j < kBinPer; ++j) {
+      const uint32_t v = t0 + j * kBinNT + threadIdx.x;
+#pragma unroll
+      for (int b = 0; b < kNumBins; ++b) {
+        const unsigned mask = __ballot_sync(kFull, bin[j] == b);
+        if (!mask) continue;
+        const uint32_t base = __shfl_sync(kFull, run, b);
+        if (lane == b) run += __popc(mask);
+        if (bin[j] != b) continue;
+        const uint32_t pos = base + __popc(mask & lt);
         D.bins[b][pos] = v;
         if (b == kNumBins - 1) {
           // the row is cut into pieces for separate blocks; the table (table passes only) is a
           // whole number of kHubChunk-slot chunks, each chunk recording its owner
           if (want_off) {
-            const uint32_t hc = cap < kHubChunk ? kHubChunk : cap;
+            const uint32_t hc = cap[j] < kHubChunk ? kHubChunk : cap[j];
             const uint32_t off = atomicAdd(&C->hub_cursor, hc);
             D.hub_off[pos] = off;
             if ((unsigned long long)off + hc <= C->arena_slots)
-              for (uint32_t j = 0; j < hc / kHubChunk; ++j) D.hub_owner[off / kHubChunk + j] = pos;
+              for (uint32_t q = 0; q < hc / kHubChunk; ++q) D.hub_owner[off / kHubChunk + q] = pos;
           }
-          const uint32_t np = (d + kHubPiece - 1) / kHubPiece;
+          const uint32_t np = (dd[j] + kHubPiece - 1) / kHubPiece;
           const uint32_t p0 = atomicAdd(&C->hub_items, np);
-          for (uint32_t k = 0; k < np; ++k) D.long_items[p0 + k] = ((unsigned long long)pos << 32) | k;
+          for (uint32_t q = 0; q < np; ++q) D.long_items[p0 + q] = ((unsigned long long)pos << 32) | q;
         }
       }
     }
-    // pass accounting for the roofline: active vertices and their entries
-    const unsigned long long de = warp_sum((unsigned long long)(bin >= 0 ? d : 0u));
-    const unsigned nv = __popc(__ballot_sync(kFull, bin >= 0));
-    if ((threadIdx.x & 31) == 0 && nv) {
-      atomicAdd(&C->act_entries, de);
+    __syncthreads();  // s_cnt is rewritten by the next tile
+  }
+  act_e = warp_sum(act_e);
+  act_v = warp_sum(act_v);
+  if (lane == 0) { s_acc[wid] = act_e; s_accv[wid] = act_v; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long e = 0;
+    uint32_t nv = 0;
+    for (int w = 0; w < NW; ++w) { e += s_acc[w]; nv += s_accv[w]; }
+    if (nv) {
+      atomicAdd(&C->act_entries, e);
       atomicAdd(&C->act_vertices, nv);
     }
   }
@@ -415,10 +491,14 @@ __device__ __forceinline__ unsigned long long cand_scan(const Dev& D, const VtxC
 // the team's lanes within the warp. BLOCK: the team is the whole block; warps take list space
 // from the shared counter *bcount (one atomic per warp and batch), which the caller reads after
 // a barrier. Otherwise the team is part of one warp and the count is returned.
+// With integer weights (WINT) each entry gathers its neighbour's (total, community) word
+// (Dev::ca) instead of the community alone, and the lane that creates a key also lists the
+// community's total (`lista`, beside the slot index), so that the evaluation half reads no
+// global memory at all.
 template <bool WINT, bool BLOCK, int NB, class Tbl>
 __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, uint32_t v, uint32_t lane,
                                                 uint32_t step, unsigned tmask, const Tbl& tbl,
-                                                uint16_t* list, uint32_t* bcount,
+                                                uint16_t* list, uint32_t* lista, uint32_t* bcount,
                                                 typename WTraits<WINT>::Acc& self_acc, uint32_t& err) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
@@ -427,7 +507,7 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
   const uint32_t lt = lanemask_lt();
   uint32_t nl = 0;
   for (uint32_t b = x.rs; b < x.re; b += NB * step) {
-    uint32_t uu[NB], cc[NB];
+    uint32_t uu[NB], cc[NB], at[NB];
     Acc ww[NB];
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
@@ -437,7 +517,16 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
       ww[k] = in ? (x.unit ? Acc(1) : (Acc)w[ek]) : Acc(0);
     }
 #pragma unroll
-    for (int k = 0; k < NB; ++k) cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+    for (int k = 0; k < NB; ++k) {
+      if constexpr (WINT) {
+        const unsigned long long y = uu[k] != v ? D.ca[uu[k]] : 0xFFFFFFFFFFFFFFFFull;
+        cc[k] = (uint32_t)y;
+        at[k] = (uint32_t)(y >> 32);
+      } else {
+        cc[k] = uu[k] != v ? D.comm[uu[k]] : kEmpty;
+        at[k] = 0;
+      }
+    }
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
       bool made = false;
@@ -458,10 +547,16 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
           uint32_t base = 0;
           if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(bcount, (uint32_t)__popc(m));
           base = __shfl_sync(kFull, base, leader);
-          if (made) list[base + __popc(m & lt)] = (uint16_t)slot;
+          if (made) {
+            list[base + __popc(m & lt)] = (uint16_t)slot;
+            if constexpr (WINT) lista[base + __popc(m & lt)] = at[k];
+          }
         }
       } else {
-        if (made) list[nl + __popc(m & lt)] = (uint16_t)slot;
+        if (made) {
+          list[nl + __popc(m & lt)] = (uint16_t)slot;
+          if constexpr (WINT) lista[nl + __popc(m & lt)] = at[k];
+        }
         nl += __popc(m);
       }
     }
@@ -473,7 +568,8 @@ __device__ __forceinline__ uint32_t insert_list(const Dev& D, const VtxCtx& x, u
 // distinct neighbouring communities (as cand_scan), emptying each slot after reading it.
 template <bool WINT, int NB, class Tbl>
 __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxCtx& x, const Tbl& tbl,
-                                                        const uint16_t* list, uint32_t i0, uint32_t nl,
+                                                        const uint16_t* list, const uint32_t* lista,
+                                                        uint32_t i0, uint32_t nl,
                                                         uint32_t step, float self_v, bool lowest) {
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
@@ -487,15 +583,19 @@ __device__ __forceinline__ unsigned long long list_scan(const Dev& D, const VtxC
       const uint32_t ik = i + k * step;
       cc[k] = kEmpty;
       vv[k] = Acc(0);
+      ac[k] = 0.0;
       if (ik < nl) {
         const uint32_t sl = list[ik];
         tbl.load(sl, cc[k], vv[k]);
         tbl.clear(sl);
+        if constexpr (WINT) ac[k] = (double)lista[ik];
       }
       if (cc[k] == x.cv) cc[k] = kEmpty;
     }
+    if constexpr (!WINT) {
 #pragma unroll
-    for (int k = 0; k < NB; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
+      for (int k = 0; k < NB; ++k) ac[k] = cc[k] != kEmpty ? D.a[cc[k]] : 0.0;
+    }
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
       if (cc[k] == kEmpty) continue;
@@ -535,13 +635,16 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
   constexpr int TEAMS = 256 / T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int team = threadIdx.x / T, lane = threadIdx.x % T;
-  // per team: a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 u16
-  // slot indices (table capacities stay below 2^16: they must fit shared memory)
+  // per team: a table of `cap` slots (packed u64, or u32 keys + sums), a list of cap / 2 u16
+  // slot indices (table capacities stay below 2^16: they must fit shared memory) and, with
+  // integer weights, the cap / 2 listed communities' totals (u32)
   constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + (size_t)team * cap;
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)TEAMS * cap * sizeof(uint32_t)) + (size_t)team * cap;
   unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)team * cap;
   uint16_t* list = reinterpret_cast<uint16_t*>(smem + (size_t)TEAMS * cap * kSlotBytes) + (size_t)team * (cap / 2);
+  // integer weights: the listed communities' totals, cap / 2 u32 per team after the lists
+  uint32_t* lista = reinterpret_cast<uint32_t*>(smem + (size_t)TEAMS * cap * (kSlotBytes + 1)) + (size_t)team * (cap / 2);
 
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
@@ -580,17 +683,17 @@ __global__ void __launch_bounds__(256, 4) k_opt_team(int dslot, int bin, uint32_
       // still cost their instructions
       const int nb = batch_for(x.re - x.rs, T);
       if (live) {
-        if (nb == 1) nl = insert_list<WINT, false, 1>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
-        else if (nb == 2) nl = insert_list<WINT, false, 2>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
-        else nl = insert_list<WINT, false, kBatch>(D, x, v, lane, T, tmask, tbl, list, nullptr, self_acc, err);
+        if (nb == 1) nl = insert_list<WINT, false, 1>(D, x, v, lane, T, tmask, tbl, list, lista, nullptr, self_acc, err);
+        else if (nb == 2) nl = insert_list<WINT, false, 2>(D, x, v, lane, T, tmask, tbl, list, lista, nullptr, self_acc, err);
+        else nl = insert_list<WINT, false, kBatch>(D, x, v, lane, T, tmask, tbl, list, lista, nullptr, self_acc, err);
       }
       self_acc = team_sum<T>(self_acc);
       __syncwarp();
       if (live) {
         const float self_v = Tr::to_float(self_acc);
-        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, lane, nl, T, self_v, lowest);
-        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, lane, nl, T, self_v, lowest);
-        else best = list_scan<WINT, kBatch>(D, x, tbl, list, lane, nl, T, self_v, lowest);
+        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, lista, lane, nl, T, self_v, lowest);
+        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, lista, lane, nl, T, self_v, lowest);
+        else best = list_scan<WINT, kBatch>(D, x, tbl, list, lista, lane, nl, T, self_v, lowest);
       }
       best = team_max<T>(best, kFull);
       __syncwarp();  // the listed slots are empty again before the next vertex inserts
@@ -659,12 +762,14 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
   __shared__ unsigned long long red_best[2][NW];
   __shared__ Acc red_self[2][NW];
   __shared__ uint32_t nlist[2];
-  // a table of `cap` slots (packed u64, or u32 keys + sums) and a list of cap / 2 u16 slot indices
+  // a table of `cap` slots (packed u64, or u32 keys + sums), a list of cap / 2 u16 slot indices
+  // and, with integer weights, the listed communities' totals (cap / 2 u32)
   constexpr size_t kSlotBytes = WINT ? 8 : 4 + sizeof(Acc);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
   Acc* vals = reinterpret_cast<Acc*>(smem + (size_t)cap * sizeof(uint32_t));
   unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
   uint16_t* list = reinterpret_cast<uint16_t*>(smem + (size_t)cap * kSlotBytes);
+  uint32_t* lista = reinterpret_cast<uint32_t*>(smem + (size_t)cap * (kSlotBytes + 1));  // integer weights
   Ctrl* C = D.ctrl;
   const uint32_t count = C->bin_count[bin];
   if (blockIdx.x >= count) return;  // (block-uniform)
@@ -698,9 +803,9 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
       tbl.shift = 32u - log2_pow2(cap_v);
       Acc self_acc = Acc(0);  // the own community's weight, kept out of the table
       if (ok) {
-        if (nb == 1) insert_list<WINT, true, 1>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
-        else if (nb == 2) insert_list<WINT, true, 2>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
-        else insert_list<WINT, true, kBatch>(D, x, v, threadIdx.x, NT, kFull, tbl, list, &nlist[par], self_acc, err);
+        if (nb == 1) insert_list<WINT, true, 1>(D, x, v, threadIdx.x, NT, kFull, tbl, list, lista, &nlist[par], self_acc, err);
+        else if (nb == 2) insert_list<WINT, true, 2>(D, x, v, threadIdx.x, NT, kFull, tbl, list, lista, &nlist[par], self_acc, err);
+        else insert_list<WINT, true, kBatch>(D, x, v, threadIdx.x, NT, kFull, tbl, list, lista, &nlist[par], self_acc, err);
       }
       self_acc = warp_sum(self_acc);
       if (lane == 0) red_self[par][wid] = self_acc;
@@ -711,9 +816,9 @@ __global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32
       const uint32_t nl = nlist[par];
       const float self_v = Tr::to_float(self_all);
       if (ok) {
-        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
-        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
-        else best = list_scan<WINT, kBatch>(D, x, tbl, list, threadIdx.x, nl, NT, self_v, lowest);
+        if (nb == 1) best = list_scan<WINT, 1>(D, x, tbl, list, lista, threadIdx.x, nl, NT, self_v, lowest);
+        else if (nb == 2) best = list_scan<WINT, 2>(D, x, tbl, list, lista, threadIdx.x, nl, NT, self_v, lowest);
+        else best = list_scan<WINT, kBatch>(D, x, tbl, list, lista, threadIdx.x, nl, NT, self_v, lowest);
       }
       if (threadIdx.x == 0) nlist[par ^ 1] = 0;  // the next vertex's count (read by no one now)
     }
