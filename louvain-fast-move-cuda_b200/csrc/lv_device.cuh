@@ -275,7 +275,7 @@ __device__ __forceinline__ int table_add_at(uint32_t* keys, Acc* vals, uint32_t 
       slot = h;
       return made;
     }
-    h = (h + 1) & mask;
+    h = (h + probe + 1u) & mask;  // triangular steps (see PackedTable::add_at)
   }
   return 0;
 }
@@ -369,7 +369,11 @@ struct PackedTable {
         slot = h;
         return 1;
       }
-      h = (h + 1) & mask;
+      // triangular steps (offsets 1, 3, 6, ... from the home slot): they visit every slot of a
+      // power-of-two table within `mask + 1` probes and break up the runs of occupied slots that
+      // linear probing builds, so the longest probe of a warp's inserts -- the one every lane
+      // waits for -- stays short
+      h = (h + probe + 1u) & mask;
     }
     return 0;
   }
