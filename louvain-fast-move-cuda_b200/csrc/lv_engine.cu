@@ -170,6 +170,10 @@ static const int32_t kTuneCandidates[][7] = {
 };
 constexpr int kTuneN = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
 static const int kTeamT[6] = {4, 8, 16, 32, 32, 32};
+// Lanes per vertex of the gain kernels' short-row bins: a quarter of the contraction's, so each
+// lane takes up to four entries of its row (kBatch) and a warp works on four times as many
+// vertices at once, sharing the per-vertex instructions among them.
+static const int kOptT[6] = {1, 2, 4, 8, 32, 32};
 
 struct Block {
   void* p;
@@ -344,7 +348,7 @@ class Run {
     if ((size_t)block_cap * slot > (size_t)max_smem - 1024 || block_cap > 65536)
       throw Fail{LV_ERR_ARGUMENT, "bin 6 table does not fit shared memory"};
     for (int b = 0; b < 6; ++b)
-      if ((size_t)(256 / kTeamT[b]) * team_cap[b] * slot > (size_t)max_smem - 1024)
+      if ((size_t)(256 / std::min(kTeamT[b], kOptT[b])) * team_cap[b] * slot > (size_t)max_smem - 1024)
         throw Fail{LV_ERR_ARGUMENT, "team bin table does not fit shared memory"};
   }
 
@@ -354,9 +358,10 @@ class Run {
   size_t con_slot_bytes() const { return 4 + acc_size() + 1; }
   size_t opt_slot_bytes() const { return 4 + acc_size() + 1 + (wint ? 2 : 0); }
 
-  template <int T>
+  // T: the contraction kernel's lanes per row, TO: the gain kernel's
+  template <int T, int TO>
   void team_grid(int b, const void* opt_fn, const void* con_fn) {
-    const size_t osmem = (size_t)(256 / T) * team_cap[b] * opt_slot_bytes();
+    const size_t osmem = (size_t)(256 / TO) * team_cap[b] * opt_slot_bytes();
     const size_t csmem = (size_t)(256 / T) * team_cap[b] * con_slot_bytes();
     ensure_dyn_smem(ctx->device, opt_fn, osmem);
     ensure_dyn_smem(ctx->device, con_fn, csmem);
@@ -365,12 +370,12 @@ class Run {
 
   template <bool WI>
   void configure_kernels() {
-    team_grid<4>(0, (const void*)k_opt_team<4, WI>, (const void*)k_contract_team<4, WI>);
-    team_grid<8>(1, (const void*)k_opt_team<8, WI>, (const void*)k_contract_team<8, WI>);
-    team_grid<16>(2, (const void*)k_opt_team<16, WI>, (const void*)k_contract_team<16, WI>);
-    team_grid<32>(3, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
-    team_grid<32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
-    team_grid<32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<4, 1>(0, (const void*)k_opt_team<1, WI>, (const void*)k_contract_team<4, WI>);
+    team_grid<8, 2>(1, (const void*)k_opt_team<2, WI>, (const void*)k_contract_team<8, WI>);
+    team_grid<16, 4>(2, (const void*)k_opt_team<4, WI>, (const void*)k_contract_team<16, WI>);
+    team_grid<32, 8>(3, (const void*)k_opt_team<8, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<32, 32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<32, 32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     const size_t bsmem = (size_t)block_cap * opt_slot_bytes();
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, (size_t)block_cap * con_slot_bytes());
@@ -700,10 +705,10 @@ class Run {
     if (!gc.on) LV_CUDA(cudaEventRecord(ev[4], st));  // no event nodes inside captured loops
     k_chunk_flags<<<grid_n, 256, 0, st>>>(Dd);
     k_bin_vertices<<<grid_n, 256, 0, st>>>(Dd, bins, WI ? 1 : 0);
-    k_opt_team<4, WI><<<grid_team[0], 256, (256 / 4) * team_cap[0] * slot, st>>>(Dd, 0, team_cap[0]);
-    k_opt_team<8, WI><<<grid_team[1], 256, (256 / 8) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
-    k_opt_team<16, WI><<<grid_team[2], 256, (256 / 16) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
-    k_opt_team<32, WI><<<grid_team[3], 256, (256 / 32) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
+    k_opt_team<1, WI><<<grid_team[0], 256, (256 / 1) * team_cap[0] * slot, st>>>(Dd, 0, team_cap[0]);
+    k_opt_team<2, WI><<<grid_team[1], 256, (256 / 2) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
+    k_opt_team<4, WI><<<grid_team[2], 256, (256 / 4) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
+    k_opt_team<8, WI><<<grid_team[3], 256, (256 / 8) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
     k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
     k_opt_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
