@@ -170,10 +170,11 @@ static const int32_t kTuneCandidates[][7] = {
 };
 constexpr int kTuneN = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
 static const int kTeamT[6] = {4, 8, 16, 32, 32, 32};
-// Lanes per vertex of the gain kernels' short-row bins: a quarter of the contraction's, so each
-// lane takes up to four entries of its row (kBatch) and a warp works on four times as many
-// vertices at once, sharing the per-vertex instructions among them.
-static const int kOptT[6] = {1, 2, 4, 8, 32, 32};
+// Lanes per vertex of the gain kernels' bins: fewer than the contraction's for the short bins (a
+// quarter for rows up to 32 entries, half for rows up to 128), so each lane takes up to four
+// entries of its row per step (kBatch) and a warp works on several vertices at once, sharing
+// the per-vertex instructions among them.
+static const int kOptT[6] = {1, 2, 4, 8, 16, 32};
 
 struct Block {
   void* p;
@@ -374,7 +375,7 @@ class Run {
     team_grid<8, 2>(1, (const void*)k_opt_team<2, WI>, (const void*)k_contract_team<8, WI>);
     team_grid<16, 4>(2, (const void*)k_opt_team<4, WI>, (const void*)k_contract_team<16, WI>);
     team_grid<32, 8>(3, (const void*)k_opt_team<8, WI>, (const void*)k_contract_team<32, WI>);
-    team_grid<32, 32>(4, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
+    team_grid<32, 16>(4, (const void*)k_opt_team<16, WI>, (const void*)k_contract_team<32, WI>);
     team_grid<32, 32>(5, (const void*)k_opt_team<32, WI>, (const void*)k_contract_team<32, WI>);
     const size_t bsmem = (size_t)block_cap * opt_slot_bytes();
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
@@ -709,7 +710,7 @@ class Run {
     k_opt_team<2, WI><<<grid_team[1], 256, (256 / 2) * team_cap[1] * slot, st>>>(Dd, 1, team_cap[1]);
     k_opt_team<4, WI><<<grid_team[2], 256, (256 / 4) * team_cap[2] * slot, st>>>(Dd, 2, team_cap[2]);
     k_opt_team<8, WI><<<grid_team[3], 256, (256 / 8) * team_cap[3] * slot, st>>>(Dd, 3, team_cap[3]);
-    k_opt_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
+    k_opt_team<16, WI><<<grid_team[4], 256, (256 / 16) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
     k_opt_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
