@@ -33,6 +33,10 @@ constexpr uint32_t kGuardLevels = 1u << 16;
 
 constexpr int kMaxChunks = 1024;
 constexpr int kNumBins = 8;
+// Vertex lists of a pass: the kNumBins degree bins, plus list kHalfBin holding the bin-6 rows
+// whose table fits half of the block table (processed by 256-thread blocks, twice as many per SM).
+constexpr int kHalfBin = kNumBins;
+constexpr int kListBins = kNumBins + 1;
 constexpr int kTraceCap = 4096;
 
 // Per-graph state (one entry per graph of a batch; a single run has one).
@@ -92,7 +96,7 @@ struct Ctrl {
   uint32_t fast;               // 1 = this pass is the per-edge "fast" pass
   uint32_t rule_sort;          // 1 = lowest community wins ties, 0 = highest
   uint32_t unit_w;             // integer mode, level 0: every weight is 1, so no kernel loads w
-  uint32_t bin_count[kNumBins];
+  uint32_t bin_count[kListBins];
   uint32_t mover_count;        // movers found by team kernels: movers[0, mover_count)
   uint32_t hub_mover_count;    // movers found by block kernels: movers[n - hub_mover_count, n)
   uint32_t long_count;         // aggregation: pieces of long rows for k_hub_insert_long

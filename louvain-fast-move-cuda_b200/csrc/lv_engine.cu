@@ -381,6 +381,9 @@ class Run {
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, (size_t)block_cap * con_slot_bytes());
     grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI>, 512, bsmem));
+    // the half-block list: 256 threads, half the table
+    ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI, 256>, bsmem / 2);
+    grid_block[1] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI, 256>, 256, bsmem / 2));
   }
 
   // Upload (or copy) the input, validate it, compute k, m and the level-0 self-loop weight.
@@ -531,7 +534,7 @@ class Run {
     D.a = dalloc<double>(ctx, owned, n, st);
     D.new_comm = dalloc<uint32_t>(ctx, owned, n, st);
     D.active_it = dalloc<uint32_t>(ctx, owned, n, st);
-    for (int b = 0; b < kNumBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n, st);
+    for (int b = 0; b < kListBins; ++b) D.bins[b] = dalloc<uint32_t>(ctx, owned, n, st);
     D.hub_off = dalloc<uint32_t>(ctx, owned, n, st);
     D.hubtab = dalloc<uint32_t>(ctx, owned, n, st);
     D.hubself = dalloc<unsigned long long>(ctx, owned, n, st);
@@ -713,6 +716,7 @@ class Run {
     k_opt_team<16, WI><<<grid_team[4], 256, (256 / 16) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
     k_opt_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
     k_opt_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
+    k_opt_block<WI, 256><<<grid_block[1], 256, (block_cap / 2) * slot, st>>>(Dd, kHalfBin, block_cap / 2);
     // bin 7: rows cut into pieces over many blocks, global tables, argmax merged per vertex
     k_opt_hub_prep<WI><<<ctx->sms * 4, 256, 0, st>>>(Dd);
     k_opt_hub_scan<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
@@ -730,7 +734,7 @@ class Run {
     k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
     commit_sq();
     finalize(0, view);
-    launches += 19;
+    launches += 20;
   }
 
   // Runs one pass; returns the number of graphs still iterating.

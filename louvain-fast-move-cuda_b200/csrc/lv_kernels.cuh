@@ -28,7 +28,7 @@ struct Dev {
   double* a;            // [n] communities_weight
   uint32_t* new_comm;   // [n] target of this pass's move
   uint32_t* active_it;  // [n] pass stamp for which the vertex is active
-  uint32_t* bins[kNumBins];
+  uint32_t* bins[kListBins];  // vertex lists per degree bin (+ kHalfBin)
   uint32_t* hub_off;    // [n] arena offset per entry of the global-table bin
   uint32_t* hubtab;     // [n] aggregation: arena offset of each bin-7 new community, else kEmpty
   unsigned long long* hubself;  // [n] aggregation: self-loop weight of each bin-7 community
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kBinNT) k_bin_vertices(int dslot, BinCfg B, in
   }
   const bool want_off = !C->fast;
   constexpr int NW = kBinNT / 32;
-  __shared__ uint32_t s_cnt[NW][kNumBins];  // per warp and bin: members in this tile, then list base
+  __shared__ uint32_t s_cnt[NW][kListBins];  // per warp and bin: members in this tile, then list base
   __shared__ unsigned long long s_acc[NW];
   __shared__ uint32_t s_accv[NW];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -222,9 +222,11 @@ __global__ void __launch_bounds__(kBinNT) k_bin_vertices(int dslot, BinCfg B, in
           if (d > 0) {
             int b = bin_of(B, d);
             // a long row whose distinct communities fit the shared table stays in bin 6
-            if (b == kNumBins - 1) {
+            if (b >= kNumBins - 2) {
               cap[j] = table_cap(d, D.gid ? D.gs[g].ve - D.gs[g].vb : n);
-              if (cap[j] <= B.block_cap) b = kNumBins - 2;
+              if (b == kNumBins - 1 && cap[j] <= B.block_cap) b = kNumBins - 2;
+              // a bin-6 row whose table fits half the block table: the half-block list
+              if (b == kNumBins - 2 && 2u * cap[j] <= B.block_cap) b = kHalfBin;
             }
             bin[j] = b;
             dd[j] = d;
@@ -237,15 +239,15 @@ __global__ void __launch_bounds__(kBinNT) k_bin_vertices(int dslot, BinCfg B, in
     // members per bin in this warp (lane b keeps bin b's count)
     uint32_t mine = 0;
 #pragma unroll
-    for (int b = 0; b < kNumBins; ++b) {
+    for (int b = 0; b < kListBins; ++b) {
       uint32_t c = 0;
 #pragma unroll
       for (int j = 0; j < kBinPer; ++j) c += __popc(__ballot_sync(kFull, bin[j] == b));
       if (lane == b) mine = c;
     }
-    if (lane < kNumBins) s_cnt[wid][lane] = mine;
+    if (lane < kListBins) s_cnt[wid][lane] = mine;
     __syncthreads();
-    if (threadIdx.x < kNumBins) {
+    if (threadIdx.x < kListBins) {
       // one claim per bin for the whole tile; warps get consecutive ranges in warp order
       const int b = threadIdx.x;
       uint32_t tot = 0;
@@ -260,12 +262,12 @@ __global__ void __launch_bounds__(kBinNT) k_bin_vertices(int dslot, BinCfg B, in
       }
     }
     __syncthreads();
-    uint32_t run = lane < kNumBins ? s_cnt[wid][lane] : 0u;  // lane b: next position in bin b
+    uint32_t run = lane < kListBins ? s_cnt[wid][lane] : 0u;  // lane b: next position in bin b
 #pragma unroll
     for (int j = 0; j < kBinPer; ++j) {
       const uint32_t v = t0 + j * kBinNT + threadIdx.x;
 #pragma unroll
-      for (int b = 0; b < kNumBins; ++b) {
+      for (int b = 0; b < kListBins; ++b) {
         const unsigned mask = __ballot_sync(kFull, bin[j] == b);
         if (!mask) continue;
         const uint32_t base = __shfl_sync(kFull, run, b);
@@ -749,12 +751,14 @@ __device__ __forceinline__ unsigned long long block_max(unsigned long long x, un
 // ---- pass: optimisation, one block per high-degree vertex ----------------------------------------
 // The vertex's table lives in shared memory (capacity `cap` slots; vertices whose table would
 // not fit are in bin 7, handled by the k_opt_hub_* kernels).
-template <bool WINT>
-__global__ void __launch_bounds__(512, 2) k_opt_block(int dslot, int bin, uint32_t cap) {
+// NT threads per block: 512 for bin 6, 256 for the half-block list (tables of half the size, so
+// twice as many blocks fit an SM's shared memory and registers).
+template <bool WINT, int NT = 512>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_opt_block(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
-  constexpr int NT = 512, NW = NT / 32;
+  constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   // per-warp partials and the list count, double-buffered by vertex parity so that a vertex
   // needs two barriers (table pass) or one (fast pass): one before the keys are evaluated,
@@ -1372,7 +1376,7 @@ __global__ void __launch_bounds__(1024) k_finalize(int dslot, int single, int np
   if (threadIdx.x == 0) {
     C->n_iterating = tot;
     C->loop_continue = tot > 0;
-    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    for (int b = 0; b < kListBins; ++b) C->bin_count[b] = 0;
     C->mover_count = 0;
     C->long_movers = 0;
     C->hub_mover_count = 0;
@@ -1427,7 +1431,7 @@ __global__ void k_level_init(int dslot) {
     C->hub_mover_count = 0;
     C->hub_items = 0;
     C->apply_items = 0;
-    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    for (int b = 0; b < kListBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
     C->arena_need = 0;
     for (int i = 0; i < kMaxChunks; ++i) C->chunk_any[i] = 0;
@@ -2509,7 +2513,7 @@ __global__ void k_agg_clear_next(int dslot) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     D.newdeg[n2] = 0;
-    for (int b = 0; b < kNumBins; ++b) C->bin_count[b] = 0;
+    for (int b = 0; b < kListBins; ++b) C->bin_count[b] = 0;
     C->hub_cursor = 0;
     C->long_count = 0;  // k_hub_insert queues this aggregation's long rows from zero
     C->hub_work = 0;    // and takes its member groups from zero
