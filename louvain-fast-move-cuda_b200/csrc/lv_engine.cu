@@ -380,6 +380,7 @@ class Run {
     const size_t bsmem = (size_t)block_cap * opt_slot_bytes();
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI>, bsmem);
     ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI>, (size_t)block_cap * con_slot_bytes());
+    ensure_dyn_smem(ctx->device, (const void*)k_contract_block<WI, 256>, (size_t)(block_cap / 2) * con_slot_bytes());
     grid_block[0] = ctx->sms * std::max(1, occupancy(ctx->device, (const void*)k_opt_block<WI>, 512, bsmem));
     // the half-block list: 256 threads, half the table
     ensure_dyn_smem(ctx->device, (const void*)k_opt_block<WI, 256>, bsmem / 2);
@@ -731,7 +732,7 @@ class Run {
     k_pack_cn<<<grid_n, 256, 0, st>>>(Dd);
     k_apply<WI><<<grid_n, 256, 0, st>>>(Dd);
     k_apply_long<WI><<<grid_n, 256, 0, st>>>(Dd);
-    k_apply_hub<WI><<<ctx->sms * 4, 512, 0, st>>>(Dd);
+    k_apply_hub<WI><<<ctx->sms * 8, 256, 0, st>>>(Dd);
     commit_sq();
     finalize(0, view);
     launches += 20;
@@ -879,9 +880,10 @@ class Run {
     k_contract_team<32, WI><<<grid_team[4], 256, (256 / 32) * team_cap[4] * slot, st>>>(Dd, 4, team_cap[4]);
     k_contract_team<32, WI><<<grid_team[5], 256, (256 / 32) * team_cap[5] * slot, st>>>(Dd, 5, team_cap[5]);
     k_contract_block<WI><<<grid_block[0], 512, block_cap * slot, st>>>(Dd, 6, block_cap);
+    k_contract_block<WI, 256><<<grid_block[1], 256, (block_cap / 2) * slot, st>>>(Dd, kHalfBin, block_cap / 2);
     scan<uint32_t, false, kScanDeg>();
     k_agg_compact<WI><<<grid_n, 256, 0, st>>>(Dd);
-    launches += 14;
+    launches += 15;
   }
   void agg_tail() {
     k_agg_best<<<grid_n, 256, 0, st>>>(Dd);

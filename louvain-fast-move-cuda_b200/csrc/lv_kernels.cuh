@@ -1811,13 +1811,15 @@ __global__ void k_agg_bin(int dslot, BinCfg B) {
     if (s < n2) {
       dsum = (uint32_t)D.cd[s + 1] - (uint32_t)D.cd[s];
       bin = bin_of(B, dsum);
-      if (bin == kNumBins - 1) {
+      if (bin >= kNumBins - 2) {
         const uint32_t g = D.gid ? D.gid[D.members[(uint32_t)(D.cd[s] >> 32)]] : 0u;
-        cap = contract_cap(dsum, D.gs[g].n_next, true);
+        cap = contract_cap(dsum, D.gs[g].n_next, bin == kNumBins - 1);
+        // a bin-6 community whose table fits half the block table: the half-block list
+        if (bin == kNumBins - 2 && 2u * cap <= B.block_cap) bin = kHalfBin;
       }
     }
 #pragma unroll
-    for (int b = 0; b < kNumBins; ++b) {
+    for (int b = 0; b < kListBins; ++b) {
       const uint32_t pos = warp_append(bin, b, &C->bin_count[b]);
       if (pos != kEmpty) {
         D.bins[b][pos] = s;
@@ -2013,7 +2015,8 @@ __global__ void __launch_bounds__(256) k_hub_insert_long(int dslot) {
     Acc self_acc = Acc(0);
     // one entry per thread and step: batching the loads and inserts of several entries (or
     // trying the CAS before reading the slot) measured slower here -- more atomics in flight on
-    // the hot keys of a large community's table
+    // the hot keys of a large community's table; so did summing each 2048-entry chunk in a
+    // shared-memory table before adding its distinct keys to the global table
     for (uint32_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
       const uint32_t d = D.new_comm[D.col[e]];
       const Acc wv = unit ? Acc(1) : (Acc)w[e];
@@ -2247,13 +2250,13 @@ __global__ void __launch_bounds__(256) k_contract_team(int dslot, int bin, uint3
 }
 
 // One block per new community of bin 6 (shared-memory table, listed keys as above).
-template <bool WINT>
-__global__ void __launch_bounds__(512) k_contract_block(int dslot, int bin, uint32_t cap) {
+// NT threads per block: 512 for bin 6, 256 for the half-table list (as k_opt_block).
+template <bool WINT, int NT = 512>
+__global__ void __launch_bounds__(NT) k_contract_block(int dslot, int bin, uint32_t cap) {
   const Dev& D = c_dev[dslot];
   using Tr = WTraits<WINT>;
   using Acc = typename Tr::Acc;
   using Wt = typename Tr::W;
-  constexpr int NT = 512;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t shu[33];
   __shared__ double shd[33];
