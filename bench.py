@@ -618,18 +618,25 @@ def run_ingest(args, local):
 def system_summaries(args, local):
     """Compact records of the two systems workloads beside the default line: the 4,096-graph
     batch (2 timed steps, built-in bins) against its loop of single calls, and the served
-    stream at its saturated rate (2,000 requests/s, pool of 64) against its loop."""
+    stream at its saturated rate (2,000 requests/s, pool of 64) against its loop. Each runs in
+    a process of its own (`bench.py --workload ...`), as a user would run it, so that neither
+    inherits the device memory the default line's run and the other workload left cached."""
     out = {}
-    for name, fn, over in (
-            ("batched", run_batched, {"steps": 2, "warmup": 1, "graphs": 4096, "no_autotune": True,
-                                      "reference_loop": True}),
-            ("served", run_served, {"rates": "2000", "pool": 64, "slots": 16, "no_autotune": True,
-                                    "captured": -1, "reference_loop": True})):
+    for name, argv in (
+            ("batched", ["--workload", "batched", "--steps", "2", "--warmup", "1", "--graphs", "4096",
+                         "--no-autotune", "--reference-loop"]),
+            ("served", ["--workload", "served", "--rates", "2000", "--pool", "64", "--slots", "16",
+                        "--no-autotune", "--reference-loop"])):
         a = argparse.Namespace(**vars(args))
-        for k, v in over.items():
-            setattr(a, k, v)
+        a.steps, a.warmup = (2, 1) if name == "batched" else (args.steps, args.warmup)
+        env = dict(os.environ, LOCAL_RANK=str(local))
         try:
-            r = fn(a, local, emit=False)
+            p = subprocess.run([sys.executable, os.path.abspath(__file__), *argv], env=env,
+                               capture_output=True, text=True, timeout=1800)
+            lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+            if p.returncode != 0 or not lines:
+                raise RuntimeError(f"exit {p.returncode}: {p.stderr.strip()[-200:]}")
+            r = json.loads(lines[-1])
         except Exception as e:  # the headline line must still print
             out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
             continue
